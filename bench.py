@@ -1,0 +1,394 @@
+"""Benchmark: RK4 steps/s of the pseudo-spectral Navier-Stokes step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 256] [--impl b200|reference]
+
+Workload (the 256^3 configuration of the headline metric): Taylor-Green
+vortex 256^3, float64, nu = 1/3000, dt = 0.0025, synthetic (analytic) initial
+field.  A step is one full RK4 step (20 kernel launches, four stages of five
+passes).  The working set (~2.6 GB) is far larger than the 126 MB L2, so no
+explicit flush is needed between steps.
+
+value   : steps/s with the state resident in HBM, CUDA events on the
+          library's stream around exactly K steps (max over ranks; N > 1 runs
+          N independent replicas, one per GPU, value = N * steps / max time).
+e2e     : the same run as the `dns` CLI performs it through the C ABI with
+          host buffers: pinned host field -> dns_set_velocity, K steps with
+          dns_diagnostics every 10 steps (D2H), dns_get_fields at the end.
+roofline: the kernel with the largest share of the step, algorithmic bytes
+          per launch / its mean CUDA-event duration (dns_time_kernels).
+cpu_baseline: the reference main.c (oracle/_ref/dns, compiled against the
+          project's FFTW-subset shim since FFTW is absent) or the C
+          restatement, timed on the host cores on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NU = 1.0 / 3000.0
+DT = 0.0025
+METRIC = "256^3 RK4 steps/s (FP64 Taylor-Green, nu=1/3000, dt=0.0025)"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
+
+
+# algorithmic HBM traffic per launch of each pass, in units of one complex
+# half-spectrum field (n*n*(n/2+1)*16 bytes) and one real field (n^3 * 8)
+# [stage][pass] -> (complex fields moved, real fields moved)
+def pass_units(pressure: bool = False):
+    u = []
+    for s in range(4):
+        a = (3 + 5, 0)
+        b = (5 + 6, 0) if s == 0 else (5 + 7, 0)
+        if s == 0:
+            c = (6 + 3, 3)
+        elif s < 3:
+            c = (7 + 3, 0)
+        else:
+            c = (7 + 3, 3)
+        d = (3 + 3, 0)
+        if s == 0:
+            e = (3 + 3 + 6, 0)
+        elif s < 3:
+            e = (3 + 9 + 6, 0)
+        else:
+            e = (3 + 6 + 3 + (1 if pressure else 0), 0)
+        u.append([a, b, c, d, e])
+    return u
+
+
+def pass_bytes(n: int):
+    cf = n * n * (n // 2 + 1) * 16
+    rf = n ** 3 * 8
+    return [[uc * cf + ur * rf for (uc, ur) in st] for st in pass_units()]
+
+
+def step_bytes_model(n: int) -> int:
+    """B_step = 216 * n^2 (n/2 + 1) * 2 * 8 bytes: the minimal fused five-pass
+    traffic model of the reference path (for the % of HBM roofline figure)."""
+    return 216 * n * n * (n // 2 + 1) * 2 * 8
+
+
+def load_peak():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            a = [x.strip() for x in line.split(",")]
+            if len(a) < 9:
+                continue
+            try:
+                sm.append(float(a[1]))
+                smax = float(a[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, a[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_rate(n: int, budget_s: float = 25.0):
+    """Steps/s of the reference's CPU implementation on this host: the
+    reference main.c on the oracle's FFT (oracle/_ref/dns) when it exists,
+    else the C restatement.  Bounded sample: one untimed step, then as many
+    steps as fit the budget."""
+    import numpy as np
+
+    import dns_b200
+    import oracle
+
+    cores = os.cpu_count() or 1
+    U, V, W, P = dns_b200.tgv_fields(n)
+    if os.path.exists(oracle.REF_DNS):
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        with tempfile.TemporaryDirectory() as tmp:
+            raw = os.path.join(tmp, "tgv.raw")
+            dns_b200.write_raw(raw, (U, V, W, P))
+
+            def run(k):
+                T = "%.17g" % (DT * (k - 0.5))  # exactly k steps
+                t0 = time.perf_counter()
+                subprocess.run([oracle.REF_DNS, "-i", raw, "-n", repr(NU), "-s", repr(DT), "-t", T],
+                               check=True, env=env, stdout=subprocess.DEVNULL)
+                return time.perf_counter() - t0
+
+            t1 = run(1)
+            t2 = run(2)
+            per = max(t2 - t1, 1e-3)
+            k = max(2, min(20, int(budget_s / per)))
+            tk = run(1 + k)
+            rate = k / (tk - t1)
+            return rate, cores, "reference", (
+                f"main.c (reference, unchanged) on the oracle's FFTW-subset FFT, {n}^3 TGV, "
+                f"{k} steps timed as the difference of a {1 + k}-step and a 1-step run, "
+                f"OMP_NUM_THREADS={cores}")
+    oracle.set_threads(cores)
+    o = oracle.Oracle(n)
+    o.set_velocity(U, V, W)
+    t0 = time.perf_counter()
+    o.step(NU, DT, 1)
+    per = time.perf_counter() - t0
+    k = max(1, min(20, int(budget_s / per)))
+    t0 = time.perf_counter()
+    o.step(NU, DT, k)
+    rate = k / (time.perf_counter() - t0)
+    return rate, cores, "port", f"C restatement of main.c, {n}^3 TGV, {k} steps, {cores} threads"
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    rate, cores, kind, sample = cpu_reference_rate(args.n)
+    line = {
+        "impl": "reference", "metric": METRIC if args.n == 256 else METRIC.replace("256^3", f"{args.n}^3"),
+        "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 / rate, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"taylor-green {args.n}^3 fp64 nu=1/3000 dt=0.0025",
+                   "n": args.n, "nu": NU, "dt": DT},
+        "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+
+    import numpy as np
+    import torch
+
+    import dns_b200
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    n = args.n
+    U, V, W, _ = dns_b200.tgv_fields(n)
+    ctx = dns_b200.Context(n)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ctx.set_velocity(U, V, W)
+    ctx.step(NU, DT, args.warmup)
+    ctx.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    # -- device-resident throughput --
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        gpu_id = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        gpu_id = str(local)
+    clocks = ClockSampler(gpu_id)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.step(NU, DT, args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    barrier()
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_per_s = args.steps / (ms / 1000.0)
+    value = steps_per_s * world
+
+    # -- per-kernel timing for the roofline --
+    kms = ctx.time_kernels(NU, DT, 3).reshape(4, 5)
+    pb = pass_bytes(n)
+    share = kms.sum(axis=0)
+    dom = int(np.argmax(share))
+    dom_bytes = sum(pb[s][dom] for s in range(4)) / 4.0
+    dom_ms = float(kms[:, dom].mean())
+    peak, peak_kind = load_peak()
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(TRAFFIC) as f:
+            tj = json.load(f)
+        traffic = tj.get(str(n), {}).get(dns_b200.PASS_NAMES[dom])
+    except Exception:
+        pass
+    step_bytes = sum(map(sum, pb))
+
+    # -- end to end through the C ABI with host buffers --
+    pinned = [torch.from_numpy(a.reshape(-1)).pin_memory() for a in (U, V, W)]
+    outs = [torch.empty(n ** 3, dtype=torch.float64).pin_memory() for _ in range(3)]
+    with dns_b200.Context(n) as c2:
+        s2 = torch.cuda.ExternalStream(c2.stream)
+        c2.set_velocity(*[p.numpy() for p in pinned])
+        c2.step(NU, DT, 2)
+        c2.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s2)
+        c2.set_velocity(*[p.numpy() for p in pinned])
+        done, ndiag = 0, 0
+        while done < args.steps:
+            c2.diagnostics_dd()
+            ndiag += 1
+            k = min(10, args.steps - done)
+            c2.step(NU, DT, k)
+            done += k
+        c2.diagnostics_dd()
+        ndiag += 1
+        lib = dns_b200.load_library()
+        import ctypes
+
+        st = lib.dns_get_fields(c2._h, *[ctypes.c_void_p(o.data_ptr()) for o in outs], None)
+        assert st == 0
+        e1.record(s2)
+        e1.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        wall = time.perf_counter() - t0
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = args.steps / (e2e_ms / 1000.0) * world
+    h2d = 3 * n ** 3 * 8 / args.steps
+    d2h = (3 * n ** 3 * 8 + 32 * ndiag) / args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, cores, kind, sample = cpu_reference_rate(n)
+            cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample}
+        except Exception as ex:  # the CPU leg is a reported baseline only
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC if n == 256 else METRIC.replace("256^3", f"{n}^3"),
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"taylor-green {n}^3 fp64 nu=1/3000 dt=0.0025", "n": n,
+                       "nu": NU, "dt": DT, "precision": "fp64",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set %.2f GB >> 126 MB L2, no flush" % (ctx.info()["device_bytes"] / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": dns_b200.PASS_NAMES[dom], "peak_source": peak_kind,
+                         "kernel_ms": dom_ms, "kernel_bytes": dom_bytes},
+            "step_hbm": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes * steps_per_s / 1e9,
+                         "model_bytes_216C": step_bytes_model(n),
+                         "frac_of_model_roofline": step_bytes_model(n) * steps_per_s / (peak * 1e9)},
+            "kernel_ms": {dns_b200.PASS_NAMES[p]: [float(kms[s, p]) for s in range(4)] for p in range(5)},
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "wall_s": wall},
+            "gpu_launches": 20 * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,267 @@
+"""dns_b200 -- B200 (sm_100a) pseudo-spectral RK4 stepper, a drop-in for the
+time-stepping path of slitvinov/dns main.c.
+
+This module is the Python mirror of the C ABI in include/dns_b200.h (ctypes
+over dns_b200/lib/libdns_b200.so).  The same library backs the C command-line
+drop-in dns_b200/bin/dns.  There is no CPU fallback: every call runs the CUDA
+kernels, and importing the bindings fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libdns_b200.so")
+CLI_PATH = os.path.join(HERE, "bin", "dns")
+
+DNS_OK = 0
+DNS_ERR_ARG = 1
+DNS_ERR_UNSUPPORTED = 2
+DNS_ERR_CUDA = 3
+DNS_ERR_NOMEM = 4
+DNS_ERR_NONFINITE = 5
+DNS_ERR_STATE = 6
+DNS_PREC_FP64 = 0
+DNS_FLAG_PRESSURE = 1
+
+SUPPORTED_N = (8, 16, 32, 64, 128, 256, 512)
+KERNELS_PER_STEP = 20
+PASS_NAMES = ("A:x-inverse", "B:y-inverse", "C:z-fused", "D:y-forward", "E:x-forward+update")
+
+
+class DNSError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_long),
+        ("precision", ctypes.c_int),
+        ("flags", ctypes.c_uint),
+        ("device_bytes", ctypes.c_size_t),
+        ("slot_bytes", ctypes.c_size_t),
+        ("kernels_per_step", ctypes.c_int),
+    ]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_SIGS = {
+    "dns_create": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(_P)]),
+    "dns_destroy": (ctypes.c_int, [_P]),
+    "dns_set_velocity": (ctypes.c_int, [_P, _P, _P, _P]),
+    "dns_step": (ctypes.c_int, [_P, _D, _D, ctypes.c_long]),
+    "dns_diagnostics": (ctypes.c_int, [_P] + [ctypes.POINTER(_D)] * 4),
+    "dns_get_fields": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "dns_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+    "dns_last_error": (ctypes.c_char_p, []),
+    "dns_get_spectral": (ctypes.c_int, [_P, _P]),
+    "dns_set_spectral": (ctypes.c_int, [_P, _P]),
+    "dns_get_stale": (ctypes.c_int, [_P, _P]),
+    "dns_set_stale": (ctypes.c_int, [_P, _P]),
+    "dns_get_info": (ctypes.c_int, [_P, ctypes.POINTER(_Info)]),
+    "dns_get_stream": (_P, [_P]),
+    "dns_synchronize": (ctypes.c_int, [_P]),
+    "dns_time_kernels": (ctypes.c_int, [_P, _D, _D, ctypes.c_long, ctypes.POINTER(_D)]),
+}
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libdns_b200.so and declare the C ABI.  Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python -m dns_b200.build` "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(st: int) -> None:
+    if st != DNS_OK:
+        lib = load_library()
+        raise DNSError(st, f"{lib.dns_strerror(st).decode()}: {lib.dns_last_error().decode()}")
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One simulation on one GPU (mirror of dns_ctx in include/dns_b200.h)."""
+
+    def __init__(self, n: int, precision: int = DNS_PREC_FP64, flags: int = 0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self._lib.dns_create(n, precision, flags, ctypes.byref(h)))
+        self._h = h
+        self.n = int(n)
+        self.nf = self.n // 2 + 1
+        self.flags = flags
+
+    # -- lifetime --
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dns_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the path --
+    def set_velocity(self, U, V, W) -> None:
+        U, V, W = _f64(U), _f64(V), _f64(W)
+        for a in (U, V, W):
+            if a.size != self.n ** 3:
+                raise ValueError("velocity component must have n^3 values")
+        _check(self._lib.dns_set_velocity(self._h, _ptr(U), _ptr(V), _ptr(W)))
+
+    def step(self, nu: float, dt: float, nsteps: int = 1) -> None:
+        _check(self._lib.dns_step(self._h, nu, dt, nsteps))
+
+    def diagnostics_dd(self) -> Tuple[float, float, float, float]:
+        v = [ctypes.c_double() for _ in range(4)]
+        st = self._lib.dns_diagnostics(self._h, *[ctypes.byref(x) for x in v])
+        if st not in (DNS_OK, DNS_ERR_NONFINITE):
+            _check(st)
+        return tuple(x.value for x in v)
+
+    def diagnostics(self) -> Tuple[np.longdouble, np.longdouble]:
+        """Energy and enstrophy exactly as main.c:257-266 prints them."""
+        eh, el, oh, ol = self.diagnostics_dd()
+        return scale_diagnostics(eh, el, oh, ol, self.n)
+
+    def get_fields(self, pressure: bool = False):
+        n3 = self.n ** 3
+        out = [np.empty(n3) for _ in range(4 if pressure else 3)]
+        ptrs = [_ptr(a) for a in out] + [None] * (4 - len(out))
+        _check(self._lib.dns_get_fields(self._h, *ptrs))
+        return [a.reshape(self.n, self.n, self.n) for a in out]
+
+    def get_spectral(self) -> np.ndarray:
+        out = np.empty((3, self.n, self.n, self.nf), dtype=np.complex128)
+        _check(self._lib.dns_get_spectral(self._h, _ptr(out)))
+        return out
+
+    def set_spectral(self, uh) -> None:
+        uh = np.ascontiguousarray(uh, dtype=np.complex128)
+        if uh.shape != (3, self.n, self.n, self.nf):
+            raise ValueError("spectral state must be (3, n, n, n/2+1)")
+        _check(self._lib.dns_set_spectral(self._h, _ptr(uh)))
+
+    def get_stale(self) -> np.ndarray:
+        out = np.empty((3, self.n, self.n, self.n))
+        _check(self._lib.dns_get_stale(self._h, _ptr(out)))
+        return out
+
+    def set_stale(self, u) -> None:
+        u = _f64(u)
+        if u.size != 3 * self.n ** 3:
+            raise ValueError("stale velocity must have 3 n^3 values")
+        _check(self._lib.dns_set_stale(self._h, _ptr(u)))
+
+    # -- measurement --
+    @property
+    def stream(self) -> int:
+        return int(self._lib.dns_get_stream(self._h) or 0)
+
+    def synchronize(self) -> None:
+        _check(self._lib.dns_synchronize(self._h))
+
+    def info(self) -> dict:
+        i = _Info()
+        _check(self._lib.dns_get_info(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in _Info._fields_}
+
+    def time_kernels(self, nu: float, dt: float, nsteps: int) -> np.ndarray:
+        ms = (ctypes.c_double * KERNELS_PER_STEP)()
+        _check(self._lib.dns_time_kernels(self._h, nu, dt, nsteps, ms))
+        return np.array(list(ms))
+
+
+def scale_diagnostics(eh, el, oh, ol, n):
+    """main.c:265-266: long double sums times (double) invn3 * invn3."""
+    invn3 = 1.0 / (n * n * n)
+    s = np.longdouble(invn3 * invn3)
+    return (np.longdouble(eh) + np.longdouble(el)) * s, (np.longdouble(oh) + np.longdouble(ol)) * s
+
+
+def format_line(tstep: int, t: float, E, Om) -> str:
+    """The stdout line of main.c:267: "% 10ld % .16e % .16Le % .16Le"."""
+    def le(x):
+        s = np.format_float_scientific(np.longdouble(x), precision=16, unique=False,
+                                       exp_digits=2)
+        return s if s.startswith("-") else " " + s
+    return "% 10d % .16e %s %s" % (tstep, t, le(E), le(Om))
+
+
+def step_schedule(T: float, dt: float):
+    """(tstep, t) of every printed line of a run: the loop of main.c:256-423
+    (print every 10 steps, stop when the accumulated t exceeds T)."""
+    out = []
+    t, tstep = 0.0, 0
+    while True:
+        if tstep % 10 == 0:
+            out.append((tstep, t))
+        if t > T:
+            return out, tstep
+        t += dt
+        tstep += 1
+
+
+def tgv_fields(n: int):
+    """Taylor-Green initial condition as tgv.py writes it (tgv.py:14-27):
+    U = sin x cos y cos z, V = -cos x sin y cos z, W = P = 0 on x_i = i 2pi/n."""
+    dx = 2 * math.pi / n
+    i = np.arange(n)
+    s, c = np.sin(dx * i), np.cos(dx * i)
+    U = np.einsum("i,j,k", s, c, c)
+    V = np.einsum("i,j,k", -c, s, c)
+    W = np.zeros((n, n, n))
+    P = np.zeros((n, n, n))
+    return U, V, W, P
+
+
+def write_raw(path: str, fields) -> None:
+    """Write a .raw file: 4 x n^3 float64, U V W P (tgv.py:19-27)."""
+    with open(path, "wb") as f:
+        for a in fields:
+            f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+
+
+def read_raw(path: str):
+    """Read a .raw file; n from the size as main.c:163-171 does."""
+    a = np.fromfile(path, dtype=np.float64)
+    n = round(float(np.float32(len(a) // 4)) ** (1.0 / 3))
+    if 4 * n ** 3 != len(a):
+        raise ValueError(f"wrong file '{path}'")
+    return n, a.reshape(4, n, n, n)

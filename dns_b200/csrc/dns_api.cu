@@ -1,0 +1,551 @@
+// dns_api.cu -- context, launch orchestration (CUDA graphs) and the C ABI
+// declared in include/dns_b200.h.
+//
+// Device memory of a context is one arena:
+//   spectral slots, each [n][n][nfp] complex double:
+//     0..2   SA   state at the start of a step (U_hat, V_hat, W_hat)
+//     3..5   SB   RK stage input (main.c's U_hat during stages 1-3)
+//     6..8   ACC  RK accumulator (main.c's U_hat1)
+//     9..15  WORK seven partially transformed fields of the stage
+//     16     P    pressure of the last stage (DNS_FLAG_PRESSURE only)
+//   stale real velocity [3][n^3] double (main.c's U, V, W between steps)
+//   twiddles, reduction partials.
+// main.c's U_hat0 is SA itself: stage 0 reads SA and writes SB/ACC, stage 3
+// writes the new state back into SA, so the copies of main.c:334-342 and
+// main.c:415-420 disappear.
+#include "dns_b200.h"
+#include "kernels.cuh"
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+using namespace dnsb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+enum { SLOT_SA = 0, SLOT_SB = 3, SLOT_ACC = 6, SLOT_WORK = 9, SLOT_P = 16, NSLOTS = 17 };
+
+int fail(int code, const char *what, const char *file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s (%s:%d)", what, file, line);
+  g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t err_ = (call);                                                       \
+    if (err_ != cudaSuccess) {                                                       \
+      return fail(DNS_ERR_CUDA, cudaGetErrorString(err_), __FILE__, __LINE__);       \
+    }                                                                                \
+  } while (0)
+
+// cos(2 pi k / n), sin(2 pi k / n): long double with octant reduction so that
+// the symmetric values (0, +-1, sqrt(1/2)) are exact, rounded once to double.
+void sincos2pi(long k, long n, double *c, double *s) {
+  const long double PI_L = 3.141592653589793238462643383279502884L;
+  k %= n;
+  if (k < 0) k += n;
+  const long q = (4 * k) / n, r = (4 * k) % n;
+  long double cc, ss;
+  if (r == 0) {
+    cc = 1.0L;
+    ss = 0.0L;
+  } else if (2 * r <= n) {
+    const long double x = (PI_L / 2.0L) * (long double)r / (long double)n;
+    cc = cosl(x);
+    ss = sinl(x);
+  } else {
+    const long double x = (PI_L / 2.0L) * (long double)(n - r) / (long double)n;
+    cc = sinl(x);
+    ss = cosl(x);
+  }
+  const double c0 = (double)cc, s0 = (double)ss;
+  switch (q) {
+    case 0: *c = c0; *s = s0; break;
+    case 1: *c = -s0; *s = c0; break;
+    case 2: *c = -c0; *s = -s0; break;
+    default: *c = s0; *s = -c0; break;
+  }
+}
+
+}  // namespace
+
+struct dns_ctx {
+  long n = 0;
+  int precision = 0;
+  unsigned flags = 0;
+  int device = 0;
+  Geo g{};
+  cudaStream_t stream = nullptr;
+  char *arena = nullptr;
+  size_t arena_bytes = 0;
+  cd *S = nullptr;        // spectral slots
+  double *stale = nullptr;
+  cd *tw = nullptr;
+  double4 *diag_part = nullptr, *diag_out = nullptr;
+  int diag_blocks = 0;
+  double4 *diag_host = nullptr;  // pinned
+  double *realbuf = nullptr;     // [4][n^3], allocated on first dns_get_fields
+  bool have_state = false;
+  cudaGraphExec_t graph = nullptr;
+  double graph_nu = 0, graph_dt = 0;
+  int kernels_per_step = 20;
+};
+
+namespace {
+
+constexpr double RK_A[4] = {1 / 6.0, 1 / 3.0, 1 / 3.0, 1 / 6.0};  // main.c:15
+constexpr double RK_B[3] = {0.5, 0.5, 1.0};                       // main.c:16
+
+ColJobs jobs_pass_a(int in0, bool first) {
+  (void)first;
+  ColJobs j;
+  for (int q = 0; q < 8; q++) j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1;
+  const int w = SLOT_WORK;
+  j.in_slot[0] = in0 + 0; j.out_slot[0] = w + SU;
+  j.in_slot[1] = in0 + 1; j.out_slot[1] = w + SV; j.der_slot[1] = w + SDVDX;
+  j.in_slot[2] = in0 + 2; j.out_slot[2] = w + SW; j.der_slot[2] = w + SDWDX;
+  return j;
+}
+ColJobs jobs_pass_b(bool first) {
+  ColJobs j;
+  for (int q = 0; q < 8; q++) j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1;
+  const int w = SLOT_WORK;
+  j.in_slot[0] = w + SU; j.out_slot[0] = w + SU; j.der_slot[0] = w + SDUDY;
+  j.in_slot[1] = w + SV; j.out_slot[1] = w + SV;
+  // the first stage reads the stale real velocity, so W itself is not needed
+  j.in_slot[2] = w + SW; j.out_slot[2] = first ? -1 : w + SW; j.der_slot[2] = w + SDWDY;
+  j.in_slot[3] = w + SDVDX; j.out_slot[3] = w + SDVDX;
+  j.in_slot[4] = w + SDWDX; j.out_slot[4] = w + SDWDX;
+  return j;
+}
+ColJobs jobs_map(const int *in, const int *out, int cnt) {
+  ColJobs j;
+  for (int q = 0; q < 8; q++) j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1;
+  for (int q = 0; q < cnt; q++) j.in_slot[q] = in[q], j.out_slot[q] = out[q];
+  return j;
+}
+
+template <int N>
+struct Ops {
+  static constexpr int W = 8;
+  static constexpr int E = Plan<N>::E;
+  static constexpr int CT = (N / E) * W;
+  static constexpr size_t COL_SMEM = (size_t)(N + N * W) * sizeof(cd);
+  static constexpr size_t UPD_SMEM = (size_t)(N + 3 * N * W) * sizeof(cd);
+  static constexpr size_t Z_SMEM = (size_t)(N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(cd);
+
+  template <class K>
+  static cudaError_t allow(K kern, size_t smem) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  static cudaError_t setup() {
+    cudaError_t e;
+    if ((e = allow(k_colpass<N, W, 0, false>, COL_SMEM))) return e;
+    if ((e = allow(k_colpass<N, W, 0, true>, COL_SMEM))) return e;
+    if ((e = allow(k_colpass<N, W, 1, false>, COL_SMEM))) return e;
+    if ((e = allow(k_colpass<N, W, 1, true>, COL_SMEM))) return e;
+    if ((e = allow(k_xfwd_update<N, W, 0>, UPD_SMEM))) return e;
+    if ((e = allow(k_xfwd_update<N, W, 1>, UPD_SMEM))) return e;
+    if ((e = allow(k_xfwd_update<N, W, 2>, UPD_SMEM))) return e;
+    if ((e = allow(k_xfwd_update<N, W, 3>, UPD_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 0>, Z_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 1>, Z_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 2>, Z_SMEM))) return e;
+    if ((e = allow(k_zr2c<N>, Z_SMEM))) return e;
+    if ((e = allow(k_zc2r<N>, Z_SMEM))) return e;
+    return cudaSuccess;
+  }
+
+  template <int AXIS, bool FWD>
+  static void colpass(dns_ctx *c, const ColJobs &jobs, int njobs) {
+    dim3 grid(c->g.nfp / W, N, njobs);
+    k_colpass<N, W, AXIS, FWD><<<grid, CT, COL_SMEM, c->stream>>>(c->S, c->S, c->tw, c->g, jobs);
+  }
+
+  static dim3 zgrid(int nfields) { return dim3((N * N) / ZCfg<N>::LINES, nfields); }
+
+  // kernel `k` (0..4) of RK stage `s`
+  static void stage_kernel(dns_ctx *c, int s, int k, double nu, double dt) {
+    const Geo &g = c->g;
+    cd *work = c->S + SLOT_WORK * g.slot;
+    const double invn3 = 1.0 / (double)g.nreal;
+    switch (k) {
+      case 0:
+        colpass<0, false>(c, jobs_pass_a(s == 0 ? SLOT_SA : SLOT_SB, s == 0), 3);
+        break;
+      case 1:
+        colpass<1, false>(c, jobs_pass_b(s == 0), 5);
+        break;
+      case 2:
+        if (s == 0)
+          k_zstage<N, 0><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+        else if (s < 3)
+          k_zstage<N, 1><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+        else
+          k_zstage<N, 2><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+        break;
+      case 3: {
+        const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+        colpass<1, true>(c, jobs_map(io, io, 3), 3);
+        break;
+      }
+      default: {
+        StageArgs sa;
+        sa.u0 = c->S + SLOT_SA * g.slot;
+        sa.us = c->S + (s == 0 ? SLOT_SA : SLOT_SB) * g.slot;
+        sa.acc = c->S + SLOT_ACC * g.slot;
+        sa.next = c->S + SLOT_SB * g.slot;
+        sa.ph = (s == 3 && (c->flags & DNS_FLAG_PRESSURE)) ? c->S + SLOT_P * g.slot : nullptr;
+        sa.nu = nu;
+        sa.dt = dt;
+        sa.a = RK_A[s];
+        sa.b = s < 3 ? RK_B[s] : 0.0;
+        dim3 grid(g.nfp / W, N);
+        switch (s) {
+          case 0: k_xfwd_update<N, W, 0><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
+          case 1: k_xfwd_update<N, W, 1><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
+          case 2: k_xfwd_update<N, W, 2><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
+          default: k_xfwd_update<N, W, 3><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
+        }
+      }
+    }
+  }
+
+  static void step(dns_ctx *c, double nu, double dt) {
+    for (int s = 0; s < 4; s++)
+      for (int k = 0; k < 5; k++) stage_kernel(c, s, k, nu, dt);
+  }
+
+  // forward transform of the three stale real slots into SA
+  static void forward(dns_ctx *c) {
+    const Geo &g = c->g;
+    cd *work = c->S + SLOT_WORK * g.slot;
+    k_zr2c<N><<<zgrid(3), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(c->stale, work, c->tw, g);
+    const int w3[3] = {SLOT_WORK + 0, SLOT_WORK + 1, SLOT_WORK + 2};
+    const int sa[3] = {SLOT_SA + 0, SLOT_SA + 1, SLOT_SA + 2};
+    colpass<1, true>(c, jobs_map(w3, w3, 3), 3);
+    colpass<0, true>(c, jobs_map(w3, sa, 3), 3);
+  }
+
+  // c2r(X) / n^3 of SA (and P) into realbuf [4][n^3]
+  static void backward(dns_ctx *c, int nfields) {
+    const Geo &g = c->g;
+    cd *work = c->S + SLOT_WORK * g.slot;
+    const int in[4] = {SLOT_SA + 0, SLOT_SA + 1, SLOT_SA + 2, SLOT_P};
+    const int w4[4] = {SLOT_WORK + 0, SLOT_WORK + 1, SLOT_WORK + 2, SLOT_WORK + 3};
+    colpass<0, false>(c, jobs_map(in, w4, nfields), nfields);
+    colpass<1, false>(c, jobs_map(w4, w4, nfields), nfields);
+    k_zc2r<N><<<zgrid(nfields), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->realbuf, c->tw, g,
+                                                                        1.0 / (double)g.nreal);
+  }
+};
+
+template <class F>
+bool dispatch(long n, F &&f) {
+  switch (n) {
+    case 8: f(Ops<8>{}); return true;
+    case 16: f(Ops<16>{}); return true;
+    case 32: f(Ops<32>{}); return true;
+    case 64: f(Ops<64>{}); return true;
+    case 128: f(Ops<128>{}); return true;
+    case 256: f(Ops<256>{}); return true;
+    case 512: f(Ops<512>{}); return true;
+    default: return false;
+  }
+}
+
+int check_launch(const char *file, int line) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(DNS_ERR_CUDA, cudaGetErrorString(e), file, line);
+  return DNS_OK;
+}
+#define CKL()                                          \
+  do {                                                 \
+    int st_ = check_launch(__FILE__, __LINE__);        \
+    if (st_ != DNS_OK) return st_;                     \
+  } while (0)
+
+int run_diag(dns_ctx *c) {
+  k_diag<256><<<c->diag_blocks, 256, 0, c->stream>>>(c->S + SLOT_SA * c->g.slot, c->g, c->diag_part);
+  k_diag_final<256><<<1, 256, 0, c->stream>>>(c->diag_part, c->diag_blocks, c->diag_out);
+  CKL();
+  return DNS_OK;
+}
+
+int build_graph(dns_ctx *c, double nu, double dt) {
+  if (c->graph && c->graph_nu == nu && c->graph_dt == dt) return DNS_OK;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  cudaGraph_t gr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  dispatch(c->n, [&](auto ops) { decltype(ops)::step(c, nu, dt); });
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &gr);
+  if (le != cudaSuccess) return fail(DNS_ERR_CUDA, cudaGetErrorString(le), __FILE__, __LINE__);
+  CK(ce);
+  cudaError_t ie = cudaGraphInstantiate(&c->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  CK(ie);
+  c->graph_nu = nu;
+  c->graph_dt = dt;
+  return DNS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dns_strerror(int status) {
+  switch (status) {
+    case DNS_OK: return "success";
+    case DNS_ERR_ARG: return "invalid argument";
+    case DNS_ERR_UNSUPPORTED: return "unsupported grid size or precision";
+    case DNS_ERR_CUDA: return "CUDA error";
+    case DNS_ERR_NOMEM: return "out of memory";
+    case DNS_ERR_NONFINITE: return "non-finite energy or enstrophy";
+    case DNS_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+  }
+}
+
+const char *dns_last_error(void) { return g_last_error.c_str(); }
+
+int dns_create(long n, int precision, unsigned flags, dns_ctx **out) {
+  if (!out) return fail(DNS_ERR_ARG, "out is NULL", __FILE__, __LINE__);
+  *out = nullptr;
+  if (precision != DNS_PREC_FP64)
+    return fail(DNS_ERR_UNSUPPORTED, "precision not supported", __FILE__, __LINE__);
+  cudaError_t se = cudaErrorInvalidValue;
+  if (!dispatch(n, [&](auto ops) { se = decltype(ops)::setup(); })) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "n = %ld is not supported (powers of two 8..512)", n);
+    return fail(DNS_ERR_UNSUPPORTED, buf, __FILE__, __LINE__);
+  }
+  CK(se);
+  dns_ctx *c = new dns_ctx();
+  c->n = n;
+  c->precision = precision;
+  c->flags = flags;
+  cudaGetDevice(&c->device);
+  Geo &g = c->g;
+  g.n = (int)n;
+  g.nf = (int)(n / 2 + 1);
+  g.nfp = (g.nf + 7) / 8 * 8;
+  g.slot = (long long)n * n * g.nfp;
+  g.nreal = (long long)n * n * n;
+  // 2/3 rule of main.c:231-238: keep |k| < kmax with kmax = 2/3 (n/2 + 1)
+  const double kmax = 2. / 3. * (n / 2 + 1);
+  int kcut = -1;
+  while ((double)(kcut + 1) < kmax) kcut++;
+  g.kcut = kcut;
+  const long long npts = (long long)n * n * g.nf;
+  c->diag_blocks = (int)((npts + 255) / 256 < 1184 ? (npts + 255) / 256 : 1184);
+
+  const size_t slot_b = (size_t)g.slot * sizeof(cd);
+  const size_t spec_b = slot_b * NSLOTS;
+  const size_t stale_b = (size_t)g.nreal * 3 * sizeof(double);
+  const size_t tw_b = (size_t)n * sizeof(cd);
+  const size_t part_b = (size_t)c->diag_blocks * sizeof(double4) + sizeof(double4);
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  c->arena_bytes = al(spec_b) + al(stale_b) + al(tw_b) + al(part_b);
+  cudaError_t e = cudaMalloc((void **)&c->arena, c->arena_bytes);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  char *p = c->arena;
+  c->S = (cd *)p; p += al(spec_b);
+  c->stale = (double *)p; p += al(stale_b);
+  c->tw = (cd *)p; p += al(tw_b);
+  c->diag_part = (double4 *)p;
+  c->diag_out = c->diag_part + c->diag_blocks;
+  int st = DNS_OK;
+  do {
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking))) break;
+    if ((e = cudaMallocHost((void **)&c->diag_host, sizeof(double4)))) break;
+    std::vector<double2> tw(n);
+    for (long k = 0; k < n; k++) {
+      double cs, sn;
+      sincos2pi(k, n, &cs, &sn);
+      tw[k] = make_double2(cs, -sn);  // exp(-2 pi i k / n)
+    }
+    if ((e = cudaMemcpyAsync(c->tw, tw.data(), tw_b, cudaMemcpyHostToDevice, c->stream))) break;
+    if ((e = cudaMemsetAsync(c->S, 0, spec_b, c->stream))) break;
+    if ((e = cudaMemsetAsync(c->stale, 0, stale_b, c->stream))) break;
+    if ((e = cudaStreamSynchronize(c->stream))) break;
+  } while (0);
+  if (e != cudaSuccess) {
+    st = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+    dns_destroy(c);
+    return st;
+  }
+  *out = c;
+  return DNS_OK;
+}
+
+int dns_destroy(dns_ctx *c) {
+  if (!c) return DNS_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->realbuf) cudaFree(c->realbuf);
+  if (c->diag_host) cudaFreeHost(c->diag_host);
+  if (c->arena) cudaFree(c->arena);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return DNS_OK;
+}
+
+int dns_set_velocity(dns_ctx *c, const double *U, const double *V, const double *W) {
+  if (!c || !U || !V || !W) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  const size_t fb = (size_t)c->g.nreal * sizeof(double);
+  CK(cudaMemcpyAsync(c->stale, U, fb, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->stale + c->g.nreal, V, fb, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->stale + 2 * c->g.nreal, W, fb, cudaMemcpyHostToDevice, c->stream));
+  dispatch(c->n, [&](auto ops) { decltype(ops)::forward(c); });
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_state = true;
+  return DNS_OK;
+}
+
+int dns_step(dns_ctx *c, double nu, double dt, long nsteps) {
+  if (!c || nsteps < 0) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  if (!c->have_state) return fail(DNS_ERR_STATE, "no velocity set", __FILE__, __LINE__);
+  if (nsteps == 0) return DNS_OK;
+  int st = build_graph(c, nu, dt);
+  if (st != DNS_OK) return st;
+  for (long s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->graph, c->stream));
+  return DNS_OK;
+}
+
+int dns_diagnostics(dns_ctx *c, double *e_hi, double *e_lo, double *om_hi, double *om_lo) {
+  if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
+  int st = run_diag(c);
+  if (st != DNS_OK) return st;
+  CK(cudaMemcpyAsync(c->diag_host, c->diag_out, sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const double4 r = *c->diag_host;
+  if (e_hi) *e_hi = r.x;
+  if (e_lo) *e_lo = r.y;
+  if (om_hi) *om_hi = r.z;
+  if (om_lo) *om_lo = r.w;
+  if (!isfinite(r.x) || !isfinite(r.z) || !isfinite(r.y) || !isfinite(r.w))
+    return fail(DNS_ERR_NONFINITE, "non-finite energy or enstrophy", __FILE__, __LINE__);
+  return DNS_OK;
+}
+
+int dns_get_fields(dns_ctx *c, double *U, double *V, double *W, double *P) {
+  if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
+  if (P && !(c->flags & DNS_FLAG_PRESSURE))
+    return fail(DNS_ERR_ARG, "P requested without DNS_FLAG_PRESSURE", __FILE__, __LINE__);
+  const size_t fb = (size_t)c->g.nreal * sizeof(double);
+  if (!c->realbuf) CK(cudaMalloc((void **)&c->realbuf, 4 * fb));
+  const int nf = P ? 4 : 3;
+  dispatch(c->n, [&](auto ops) { decltype(ops)::backward(c, nf); });
+  CKL();
+  double *dst[4] = {U, V, W, P};
+  for (int f = 0; f < nf; f++)
+    if (dst[f])
+      CK(cudaMemcpyAsync(dst[f], c->realbuf + f * c->g.nreal, fb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DNS_OK;
+}
+
+int dns_get_spectral(dns_ctx *c, double *uvw) {
+  if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  const Geo &g = c->g;
+  const size_t row = (size_t)g.nf * sizeof(cd), pitch = (size_t)g.nfp * sizeof(cd);
+  const size_t rows = (size_t)g.n * g.n;
+  for (int f = 0; f < 3; f++)
+    CK(cudaMemcpy2DAsync((char *)uvw + f * rows * row, row, c->S + (SLOT_SA + f) * g.slot, pitch, row,
+                         rows, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DNS_OK;
+}
+
+int dns_set_spectral(dns_ctx *c, const double *uvw) {
+  if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  const Geo &g = c->g;
+  const size_t row = (size_t)g.nf * sizeof(cd), pitch = (size_t)g.nfp * sizeof(cd);
+  const size_t rows = (size_t)g.n * g.n;
+  for (int f = 0; f < 3; f++)
+    CK(cudaMemcpy2DAsync(c->S + (SLOT_SA + f) * g.slot, pitch, (const char *)uvw + f * rows * row, row,
+                         row, rows, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_state = true;
+  return DNS_OK;
+}
+
+int dns_get_stale(dns_ctx *c, double *uvw) {
+  if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  CK(cudaMemcpyAsync(uvw, c->stale, (size_t)c->g.nreal * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DNS_OK;
+}
+
+int dns_set_stale(dns_ctx *c, const double *uvw) {
+  if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  CK(cudaMemcpyAsync(c->stale, uvw, (size_t)c->g.nreal * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DNS_OK;
+}
+
+int dns_get_info(dns_ctx *c, dns_info_t *info) {
+  if (!c || !info) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  info->n = c->n;
+  info->precision = c->precision;
+  info->flags = c->flags;
+  info->device_bytes = c->arena_bytes;
+  info->slot_bytes = (size_t)c->g.slot * sizeof(cd);
+  info->kernels_per_step = c->kernels_per_step;
+  return DNS_OK;
+}
+
+void *dns_get_stream(dns_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int dns_synchronize(dns_ctx *c) {
+  if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
+  CK(cudaStreamSynchronize(c->stream));
+  return DNS_OK;
+}
+
+int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) {
+  if (!c || !ms || nsteps <= 0) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  if (!c->have_state) return fail(DNS_ERR_STATE, "no velocity set", __FILE__, __LINE__);
+  const int K = c->kernels_per_step;
+  std::vector<cudaEvent_t> ev(K + 1);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  for (int k = 0; k < K; k++) ms[k] = 0.0;
+  int st = DNS_OK;
+  for (long s = 0; s < nsteps && st == DNS_OK; s++) {
+    CK(cudaEventRecord(ev[0], c->stream));
+    for (int k = 0; k < K; k++) {
+      dispatch(c->n, [&](auto ops) { decltype(ops)::stage_kernel(c, k / 5, k % 5, nu, dt); });
+      CK(cudaEventRecord(ev[k + 1], c->stream));
+    }
+    st = check_launch(__FILE__, __LINE__);
+    CK(cudaEventSynchronize(ev[K]));
+    for (int k = 0; k < K; k++) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      ms[k] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < K; k++) ms[k] /= (double)nsteps;
+  return st;
+}
+
+}  // extern "C"

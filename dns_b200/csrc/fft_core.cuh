@@ -1,0 +1,208 @@
+// fft_core.cuh -- register/shared-memory FFT building blocks for sm_100a.
+//
+// A line FFT of length L is spread over T = L/E threads; thread t holds
+// E values in registers in the "strided" distribution: register e <-> line
+// position t + T*e.  Each Stockham autosort stage of radix R (R divides E)
+// runs E/R butterflies per thread entirely on its own registers; between
+// stages the values are exchanged through shared memory.  After the last
+// stage the outputs are again in the strided distribution and in natural
+// order, so loads and stores to HBM use the same thread <-> position map.
+//
+// Conventions (FFTW's, which main.c relies on): forward = exp(-2 pi i jk/L),
+// backward = exp(+2 pi i jk/L), no normalisation.
+//
+// Twiddles come from a table tw[k] = exp(-2 pi i k / n), k in [0, n), of the
+// grid size n (generated on the host in long double and rounded once); a
+// length-L transform reads it with stride n/L.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <utility>
+
+namespace dnsb {
+
+typedef double2 cd;
+
+__device__ __forceinline__ cd cadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cd csub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cd cscale(cd a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ cd cconj(cd a) { return make_double2(a.x, -a.y); }
+// a * b
+__device__ __forceinline__ cd cmul(cd a, cd b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ cd cmulc(cd a, cd b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// i * a
+__device__ __forceinline__ cd cmul_i(cd a) { return make_double2(-a.y, a.x); }
+// multiply by the twiddle w (forward table entry) in the given direction
+template <bool FWD>
+__device__ __forceinline__ cd twmul(cd a, cd w) {
+  return FWD ? cmul(a, w) : cmulc(a, w);
+}
+
+// cos(2 pi m / 16) and sin(2 pi m / 16) for m in [0, 4]
+__host__ __device__ constexpr double c16(int m) {
+  return m == 0 ? 1.0
+         : m == 1 ? 0.92387953251128675613
+         : m == 2 ? 0.70710678118654752440
+         : m == 3 ? 0.38268343236508977173
+                  : 0.0;
+}
+
+// a * exp(-/+ 2 pi i m / 16) with exact handling of the trivial factors
+template <int M, bool FWD>
+__device__ __forceinline__ cd w16(cd a) {
+  constexpr int m = M & 15;
+  if constexpr (m == 0) {
+    return a;
+  } else if constexpr (m == 8) {
+    return make_double2(-a.x, -a.y);
+  } else if constexpr (m == 4) {  // exp(-i pi/2) = -i
+    return FWD ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+  } else if constexpr (m == 12) {  // exp(-3 i pi/2) = +i
+    return FWD ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+  } else {
+    // cos/sin of 2 pi m / 16 via quadrant symmetry
+    constexpr int q = m / 4, r = m % 4;
+    constexpr double c0 = c16(r), s0 = c16(4 - r);
+    constexpr double c = q == 0 ? c0 : q == 1 ? -s0 : q == 2 ? -c0 : s0;
+    constexpr double s = q == 0 ? s0 : q == 1 ? c0 : q == 2 ? -s0 : -c0;
+    // forward multiplies by (c - i s), backward by (c + i s)
+    if constexpr (FWD)
+      return make_double2(a.x * c + a.y * s, a.y * c - a.x * s);
+    else
+      return make_double2(a.x * c - a.y * s, a.y * c + a.x * s);
+  }
+}
+
+template <int B, int E, class F, int... I>
+__device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, B + I>{}), ...);
+}
+// calls f(integral_constant<int, i>) for i in [B, E)
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+  static_for_impl<B, E>(f, std::make_integer_sequence<int, E - B>{});
+}
+
+// In-register DFT of size R (1, 2, 4, 8, 16), natural order in and out
+// (recursive radix-2 decimation in time).
+template <int R, bool FWD>
+__device__ __forceinline__ void dft(cd (&a)[R]) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2) {
+    cd t = a[1];
+    a[1] = csub(a[0], t);
+    a[0] = cadd(a[0], t);
+  } else {
+    cd e[R / 2], o[R / 2];
+#pragma unroll
+    for (int k = 0; k < R / 2; k++) {
+      e[k] = a[2 * k];
+      o[k] = a[2 * k + 1];
+    }
+    dft<R / 2, FWD>(e);
+    dft<R / 2, FWD>(o);
+    static_for<0, R / 2>([&](auto K) {
+      constexpr int k = decltype(K)::value;
+      cd t = w16<k * (16 / R), FWD>(o[k]);
+      a[k] = cadd(e[k], t);
+      a[k + R / 2] = csub(e[k], t);
+    });
+  }
+}
+
+// Radix plans.  E = values per thread; radices multiply to L; each radix
+// divides E.
+template <int L>
+struct Plan;
+template <> struct Plan<2>   { static constexpr int E = 2,  NS = 1, R0 = 2,  R1 = 1, R2 = 1, R3 = 1; };
+template <> struct Plan<4>   { static constexpr int E = 4,  NS = 1, R0 = 4,  R1 = 1, R2 = 1, R3 = 1; };
+template <> struct Plan<8>   { static constexpr int E = 8,  NS = 1, R0 = 8,  R1 = 1, R2 = 1, R3 = 1; };
+template <> struct Plan<16>  { static constexpr int E = 16, NS = 1, R0 = 16, R1 = 1, R2 = 1, R3 = 1; };
+template <> struct Plan<32>  { static constexpr int E = 8,  NS = 2, R0 = 8,  R1 = 4, R2 = 1, R3 = 1; };
+template <> struct Plan<64>  { static constexpr int E = 8,  NS = 2, R0 = 8,  R1 = 8, R2 = 1, R3 = 1; };
+template <> struct Plan<128> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 8, R2 = 1, R3 = 1; };
+template <> struct Plan<256> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 16, R2 = 1, R3 = 1; };
+template <> struct Plan<512> { static constexpr int E = 8,  NS = 3, R0 = 8,  R1 = 8, R2 = 8, R3 = 1; };
+
+// Plans for the half-length complex FFT of the z (real) axis, one warp or
+// less per line: E <= 8 keeps registers free for the fused pointwise work.
+template <int M>
+struct ZPlan;
+template <> struct ZPlan<4>   { static constexpr int E = 4, NS = 1, R0 = 4, R1 = 1, R2 = 1, R3 = 1; };
+template <> struct ZPlan<8>   { static constexpr int E = 4, NS = 2, R0 = 4, R1 = 2, R2 = 1, R3 = 1; };
+template <> struct ZPlan<16>  { static constexpr int E = 4, NS = 2, R0 = 4, R1 = 4, R2 = 1, R3 = 1; };
+template <> struct ZPlan<32>  { static constexpr int E = 4, NS = 3, R0 = 4, R1 = 4, R2 = 2, R3 = 1; };
+template <> struct ZPlan<64>  { static constexpr int E = 4, NS = 3, R0 = 4, R1 = 4, R2 = 4, R3 = 1; };
+template <> struct ZPlan<128> { static constexpr int E = 4, NS = 4, R0 = 4, R1 = 4, R2 = 4, R3 = 2; };
+template <> struct ZPlan<256> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 4, R3 = 1; };
+
+// One Stockham stage on the strided distribution.
+//   L: line length, E: values per thread, R: radix, NSV: product of the
+//   radices of the previous stages.  Butterfly j = t + T*q (q < E/R) reads
+//   positions j + r*L/R (= registers q + r*E/R), applies the twiddles
+//   W_{NSV*R}^{(j mod NSV)*r}, runs a radix-R DFT and sends output r to
+//   position (j/NSV)*NSV*R + (j mod NSV) + r*NSV.
+// For the last stage (NSV*R == L) the destination is register q + r*E/R,
+// so no exchange is needed.  Otherwise outputs go to xbuf via idx(pos),
+// sync() is called, and the strided distribution is read back.
+template <int L, int E, int R, int NSV, bool FWD, class Idx, class Sync>
+__device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *__restrict__ tw,
+                                      const int twstride, cd *xbuf, Idx idx, Sync sync) {
+  constexpr int T = L / E;
+  constexpr int Q = E / R;
+  constexpr bool LAST = (NSV * R == L);
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    cd a[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) a[r] = v[q + r * Q];
+    const int j = t + T * q;
+    if constexpr (NSV > 1) {
+      const int jm = j % NSV;
+      // twiddle index in the length-n table: jm * r * (L / (NSV*R)) * twstride
+      const int base = jm * (L / (NSV * R)) * twstride;
+#pragma unroll
+      for (int r = 1; r < R; r++) a[r] = twmul<FWD>(a[r], tw[base * r]);
+    }
+    dft<R, FWD>(a);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; r++) v[q + r * Q] = a[r];
+    } else {
+      const int dst = (j / NSV) * NSV * R + (j % NSV);
+#pragma unroll
+      for (int r = 0; r < R; r++) xbuf[idx(dst + r * NSV)] = a[r];
+    }
+  }
+  if constexpr (!LAST) {
+    sync();
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = xbuf[idx(t + T * e)];
+    sync();
+  }
+}
+
+// Full line FFT of length L with plan P (P::E must equal E).
+template <int L, class P, bool FWD, class Idx, class Sync>
+__device__ __forceinline__ void line_fft(cd (&v)[P::E], const int t, const cd *__restrict__ tw,
+                                         const int twstride, cd *xbuf, Idx idx, Sync sync) {
+  constexpr int E = P::E;
+  stage<L, E, P::R0, 1, FWD>(v, t, tw, twstride, xbuf, idx, sync);
+  if constexpr (P::NS > 1) stage<L, E, P::R1, P::R0, FWD>(v, t, tw, twstride, xbuf, idx, sync);
+  if constexpr (P::NS > 2)
+    stage<L, E, P::R2, P::R0 * P::R1, FWD>(v, t, tw, twstride, xbuf, idx, sync);
+  if constexpr (P::NS > 3)
+    stage<L, E, P::R3, P::R0 * P::R1 * P::R2, FWD>(v, t, tw, twstride, xbuf, idx, sync);
+}
+
+// signed wavenumber of index i on an n-point axis (main.c:224-230:
+// kx[i] = i for i < n/2, i - n otherwise, so kx[n/2] = -n/2)
+__device__ __forceinline__ int kwave(int i, int n) { return i < n / 2 ? i : i - n; }
+
+}  // namespace dnsb

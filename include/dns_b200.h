@@ -1,0 +1,130 @@
+/*
+ * dns_b200.h -- C ABI of the B200 (sm_100a) pseudo-spectral RK4 stepper.
+ *
+ * Drop-in for the time-stepping path of slitvinov/dns main.c: the CLI
+ * (dns_b200/cli/dns.c) and the tests call the same library.  The reference has
+ * no library interface -- the path is inline in main() -- so every entry point
+ * below names the block of main.c it replaces.
+ *
+ * Conventions
+ *   - n is the grid size; the box is [0, 2 pi)^3 with n^3 nodes.  Supported:
+ *     n a power of two, 8 <= n <= 512.
+ *   - real fields are float64 [x][y][z] (z fastest), the .raw layout of
+ *     main.c:180-185 / tgv.py:19-27.
+ *   - spectral fields are complex float64 (re, im interleaved) on the half
+ *     spectrum [kx][ky][kz], kz in [0, n/2], the FFTW r2c layout main.c uses
+ *     (main.c:236); they are unnormalised like FFTW's r2c output.
+ *   - host pointers are borrowed for the duration of the call only; the
+ *     library owns all device memory.
+ *   - every function returns a status (DNS_OK == 0); the library never exits.
+ *   - a context owns one CUDA stream; it is not thread-safe, independent
+ *     contexts may be driven from different host threads.
+ */
+#ifndef DNS_B200_H
+#define DNS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DNS_OK = 0,
+  DNS_ERR_ARG = 1,        /* invalid argument (null pointer, bad size) */
+  DNS_ERR_UNSUPPORTED = 2,/* grid size or precision not supported */
+  DNS_ERR_CUDA = 3,       /* CUDA runtime error; see dns_last_error() */
+  DNS_ERR_NOMEM = 4,      /* device or pinned host allocation failed */
+  DNS_ERR_NONFINITE = 5,  /* diagnostics are NaN or Inf (main.c dies on
+                             SIGFPE there, main.c:49-50) */
+  DNS_ERR_STATE = 6       /* call out of order (e.g. step before velocity) */
+};
+
+enum { DNS_PREC_FP64 = 0 };
+
+/* flags for dns_create */
+enum {
+  DNS_FLAG_PRESSURE = 1u /* keep the pressure P_hat of the last RK stage so
+                            that dns_get_fields can return P (needed by the
+                            -d dump, main.c:269-279) */
+};
+
+typedef struct dns_ctx dns_ctx;
+
+/* Allocate device state for an n^3 grid and build twiddle tables.
+ * Replaces main.c:174-247 (allocations, FFTW plans, kx/kz, dealias, kk). */
+int dns_create(long n, int precision, unsigned flags, dns_ctx **out);
+
+/* Free everything owned by ctx.  Replaces main.c:424-460. */
+int dns_destroy(dns_ctx *ctx);
+
+/* Upload the initial velocity (three n^3 float64 arrays, host memory) and
+ * transform it: U_hat = r2c(U) etc.  The raw input also becomes the stale
+ * real-space velocity used by stage rk == 0 of step 0.
+ * Replaces main.c:180-185 (after fread) and main.c:249-251. */
+int dns_set_velocity(dns_ctx *ctx, const double *U, const double *V, const double *W);
+
+/* Advance nsteps RK4 steps with viscosity nu and time step dt.
+ * Replaces one iteration of main.c:334-422 per step (time and step counters,
+ * printing and the t > T test of main.c:332 stay with the caller). */
+int dns_step(dns_ctx *ctx, double nu, double dt, long nsteps);
+
+/* Energy and enstrophy of the current state, as double-double pairs:
+ *   E  = (e_hi + e_lo)  * invn3 * invn3,  Om = (om_hi + om_lo) * invn3 * invn3
+ * where the sums run over the half spectrum exactly as main.c:257-266 (no
+ * Hermitian weighting); the caller applies the scale in long double like
+ * main.c:265-266.  Returns DNS_ERR_NONFINITE (values still filled) when a sum
+ * is NaN or Inf. */
+int dns_diagnostics(dns_ctx *ctx, double *e_hi, double *e_lo, double *om_hi, double *om_lo);
+
+/* Real-space fields c2r(X_hat) / n^3 for X = U, V, W and (if the context was
+ * created with DNS_FLAG_PRESSURE) the pressure P of the last RK stage, into
+ * four n^3 float64 host arrays.  Any pointer may be NULL to skip that field.
+ * Replaces the dump transform of main.c:270-279. */
+int dns_get_fields(dns_ctx *ctx, double *U, double *V, double *W, double *P);
+
+/* Human-readable text of a status / of the last error on this thread. */
+const char *dns_strerror(int status);
+const char *dns_last_error(void);
+
+/* ---- state access (restart, parity tests) ----
+ * The full step state is (U_hat, V_hat, W_hat) plus the stale real-space
+ * velocity (main.c's U, V, W arrays between steps). */
+
+/* spectral velocity as [3][n][n][n/2+1] complex float64 (2*3*n*n*(n/2+1)
+ * doubles) */
+int dns_get_spectral(dns_ctx *ctx, double *uvw_hat);
+int dns_set_spectral(dns_ctx *ctx, const double *uvw_hat);
+/* stale real-space velocity, [3][n^3] float64 */
+int dns_get_stale(dns_ctx *ctx, double *uvw);
+int dns_set_stale(dns_ctx *ctx, const double *uvw);
+
+/* ---- introspection / measurement ---- */
+typedef struct {
+  long n;
+  int precision;
+  unsigned flags;
+  size_t device_bytes;     /* device memory held by the context */
+  size_t slot_bytes;       /* bytes of one padded spectral field */
+  int kernels_per_step;    /* kernel launches in one RK4 step */
+} dns_info_t;
+int dns_get_info(dns_ctx *ctx, dns_info_t *info);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time work
+ * with CUDA events on it. */
+void *dns_get_stream(dns_ctx *ctx);
+
+/* Wait for all work queued on the context's stream. */
+int dns_synchronize(dns_ctx *ctx);
+
+/* Time each kernel of the step: runs nsteps steps launch by launch with CUDA
+ * events between kernels and writes the mean time in milliseconds of each of
+ * the kernels_per_step launches of a step into ms[] (stage-major order:
+ * stage 0 passes A..E, stage 1 ..., stage 3).  The state advances by
+ * nsteps. */
+int dns_time_kernels(dns_ctx *ctx, double nu, double dt, long nsteps, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,62 @@
+"""Regenerate the golden fixtures in tests/golden from the reference checkout.
+
+Run in a container that has the reference sources (default /root/reference)
+and the built oracle (python -m dns_b200.build --oracle):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+Fixtures written:
+  ref_0128_<Re>.txt, ref_0256_<Re>.txt
+      the reference's own shipped stdout histories (0128/<Re>, 0256/<Re>):
+      Taylor-Green, dt = 0.0025, T = 10, nu = 1/Re, at 128^3 and 256^3.
+  tgv_l<L>.sha256
+      sha256 of the .raw file the reference tgv.py writes for level L.
+  refrun_tgv64_nu0.01_dt0.01_T1.txt
+      stdout of the reference main.c (compiled unchanged against the oracle's
+      FFTW-subset shim, oracle/_ref/dns) for config "64^3 Taylor-Green,
+      nu = 0.01, dt = 0.01, T = 1".
+  refrun_tgv32_nu0.01_dt0.01_T0.2.txt
+      same at 32^3, T = 0.2, used by the CLI parity test.
+"""
+import argparse
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_DNS = os.path.join(ROOT, "oracle", "_ref", "dns")
+RES = ("0100", "0200", "0400", "0800", "1600", "3000")
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    for size in ("0128", "0256"):
+        for re_ in RES:
+            shutil.copyfile(os.path.join(a.ref, size, re_), os.path.join(HERE, f"ref_{size}_{re_}.txt"))
+    with tempfile.TemporaryDirectory() as tmp:
+        for level in (3, 4, 5, 6):
+            raw = os.path.join(tmp, f"tgv{level}.raw")
+            subprocess.run([sys.executable, os.path.join(a.ref, "tgv.py"), "-l", str(level), "-o", raw],
+                           check=True, stderr=subprocess.DEVNULL)
+            digest = hashlib.sha256(open(raw, "rb").read()).hexdigest()
+            with open(os.path.join(HERE, f"tgv_l{level}.sha256"), "w") as f:
+                f.write(digest + "\n")
+        for level, T, name in ((6, "1", "refrun_tgv64_nu0.01_dt0.01_T1.txt"),
+                               (5, "0.2", "refrun_tgv32_nu0.01_dt0.01_T0.2.txt")):
+            raw = os.path.join(tmp, f"tgv{level}.raw")
+            out = subprocess.run([REF_DNS, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", T],
+                                 check=True, capture_output=True, text=True).stdout
+            with open(os.path.join(HERE, name), "w") as f:
+                f.write(out)
+    print("golden fixtures written to", HERE)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

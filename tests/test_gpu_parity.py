@@ -1,0 +1,263 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle
+(the restated main.c on its own FFT) and against the reference's golden
+histories.
+
+Tolerances (from the target of the port):
+  energy / enstrophy histories: 1e-12 relative
+  final fields: 1e-11 relative L2
+  single transforms / single steps: 1e-13 relative (pure FP64 roundoff)
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, random_field, read_history
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-12
+FIELD_TOL = 1e-11
+ROUND_TOL = 1e-13
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b)))
+
+
+@pytest.fixture(scope="module")
+def dns(dns_lib):
+    import dns_b200
+
+    return dns_b200
+
+
+# ---------------------------------------------------------------- transforms
+
+
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256])
+def test_r2c_matches_oracle(dns, oracle_lib, n):
+    rng = np.random.default_rng(n)
+    U, V, W = (rng.standard_normal((n, n, n)) for _ in range(3))
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        uh = ctx.get_spectral()
+        stale = ctx.get_stale()
+    for c, x in enumerate((U, V, W)):
+        ref = oracle_lib.r2c_3d(x)
+        assert np.abs(uh[c] - ref).max() <= ROUND_TOL * np.abs(ref).max()
+        assert np.array_equal(stale[c], x)  # the raw input is the first stale velocity
+
+
+def test_r2c_known_answer_n8(dns):
+    """poc/three.c pattern: r2c against a naive DFT with e^{-i}, unnormalised."""
+    n = 8
+    x = np.arange(n ** 3, dtype=np.float64).reshape(n, n, n) % 7 - 3.0
+    j = np.arange(n)
+    M = np.exp(-2j * np.pi * np.outer(j, j) / n)
+    ref = np.einsum("ai,bj,ck,ijk->abc", M, M, M, x)[..., : n // 2 + 1]
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(x, x, x)
+        uh = ctx.get_spectral()
+    assert np.abs(uh[0] - ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128])
+def test_c2r_matches_oracle_nonhermitian(dns, oracle_lib, n):
+    """c2r of arbitrary (non-Hermitian) half spectra: FFTW semantics, i.e.
+    complex inverse over x and y, then Im of kz = 0 and kz = n/2 ignored."""
+    rng = np.random.default_rng(100 + n)
+    nf = n // 2 + 1
+    X = rng.standard_normal((3, n, n, nf)) + 1j * rng.standard_normal((3, n, n, nf))
+    with dns.Context(n) as ctx:
+        ctx.set_spectral(X)
+        f = ctx.get_fields()
+    for c in range(3):
+        ref = oracle_lib.c2r_3d(X[c], n) / n ** 3
+        assert np.abs(f[c] - ref).max() <= ROUND_TOL * np.abs(ref).max()
+
+
+# ---------------------------------------------------------------- steps
+
+
+@pytest.mark.parametrize("n,steps", [(16, 1), (32, 1), (32, 3), (64, 2)])
+def test_steps_random_field_match_oracle(dns, oracle_lib, n, steps):
+    nu, dt = 0.02, 0.004
+    U, V, W = random_field(n, 7 + n)
+    o = oracle_lib.Oracle(n)
+    o.set_velocity(U, V, W)
+    o.step(nu, dt, steps)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        ctx.step(nu, dt, steps)
+        uh, stale = ctx.get_spectral(), ctx.get_stale()
+        E, Om = ctx.diagnostics()
+    Eo, Oo = o.diagnostics()
+    assert rel_l2(uh, o.get_spectral()) <= ROUND_TOL
+    assert rel_l2(stale, o.get_stale()) <= ROUND_TOL
+    assert abs(E - Eo) <= ROUND_TOL * Eo and abs(Om - Oo) <= ROUND_TOL * Oo
+
+
+def test_stale_velocity_quirk_is_reproduced(dns, oracle_lib):
+    """Stage 0 uses the real-space velocity left over from the previous
+    step's last stage (main.c:344): a state whose stale velocity is not
+    c2r(U_hat) steps differently, exactly as the oracle does."""
+    n, nu, dt = 16, 0.02, 0.004
+    U, V, W = random_field(n, 5)
+    U2, V2, W2 = random_field(n, 6)
+    o = oracle_lib.Oracle(n)
+    o.set_velocity(U, V, W)
+    o.set_stale(np.stack([U2, V2, W2]))
+    o.step(nu, dt, 1)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        ctx.set_stale(np.stack([U2, V2, W2]))
+        ctx.step(nu, dt, 1)
+        uh = ctx.get_spectral()
+    assert rel_l2(uh, o.get_spectral()) <= ROUND_TOL
+
+
+def test_tgv64_config_plain(dns, oracle_lib):
+    """64^3 Taylor-Green, nu = 0.01, dt = 0.01, T = 1 (100 steps): energy /
+    enstrophy every 10 steps against the reference main.c's own run
+    (refrun fixture) and the oracle, final fields against the oracle."""
+    n, nu, dt, T = 64, 0.01, 0.01, 1.0
+    steps, ts, Eg, Og = read_history(os.path.join(GOLDEN, "refrun_tgv64_nu0.01_dt0.01_T1.txt"))
+    sched, total = dns.step_schedule(T, dt)
+    assert total == 101 and [s for s, _ in sched] == list(steps)
+    U, V, W, _ = dns.tgv_fields(n)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        done = 0
+        for q, (tstep, t) in enumerate(sched):
+            ctx.step(nu, dt, tstep - done)
+            done = tstep
+            E, Om = ctx.diagnostics()
+            assert float(ts[q]) == t
+            assert abs(E - Eg[q]) <= E_TOL * Eg[q], (tstep, E, Eg[q])
+            assert abs(Om - Og[q]) <= E_TOL * Og[q], (tstep, Om, Og[q])
+        ctx.step(nu, dt, total - done)
+        uh, fields, stale = ctx.get_spectral(), ctx.get_fields(), ctx.get_stale()
+    o = oracle_lib.Oracle(n)
+    o.set_velocity(U, V, W)
+    o.step(nu, dt, total)
+    assert rel_l2(uh, o.get_spectral()) <= FIELD_TOL
+    assert rel_l2(np.stack(fields), o.dump_fields()[:3]) <= FIELD_TOL
+    assert rel_l2(stale, o.get_stale()) <= FIELD_TOL
+
+
+def _golden_run(dns, n, re_, nlines):
+    steps, ts, Eg, Og = read_history(os.path.join(GOLDEN, f"ref_{n:04d}_{re_}.txt"))
+    nu = float("%.16e" % (1.0 / int(re_)))
+    dt = 0.0025
+    U, V, W, _ = dns.tgv_fields(n)
+    E, Om = [], []
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        for q in range(nlines):
+            if q:
+                ctx.step(nu, dt, 10)
+            e, w = ctx.diagnostics()
+            E.append(e)
+            Om.append(w)
+    E = np.array(E, dtype=np.longdouble)
+    Om = np.array(Om, dtype=np.longdouble)
+    return np.abs(E - Eg[:nlines]) / Eg[:nlines], np.abs(Om - Og[:nlines]) / Og[:nlines]
+
+
+@pytest.mark.parametrize("re_", ["0100", "0200", "0400", "0800", "1600", "3000"])
+def test_golden_0128_t1(dns, re_):
+    """128^3 Taylor-Green against the reference's FFTW history over t in
+    [0, 1] (400 steps, 41 printed lines)."""
+    de, do = _golden_run(dns, 128, re_, 41)
+    assert de.max() <= E_TOL and do.max() <= E_TOL, (float(de.max()), float(do.max()))
+
+
+@pytest.mark.parametrize("re_", ["1600", "3000"])
+def test_golden_0256_t1(dns, re_):
+    """256^3 Taylor-Green against the reference's FFTW history, t in [0, 1]."""
+    de, do = _golden_run(dns, 256, re_, 41)
+    assert de.max() <= E_TOL and do.max() <= E_TOL, (float(de.max()), float(do.max()))
+
+
+# ---------------------------------------------------------------- errors
+
+
+def test_unsupported_n_is_an_error(dns):
+    for n in (12, 4, 1024):
+        with pytest.raises(dns.DNSError) as e:
+            dns.Context(n)
+        assert e.value.status == dns.DNS_ERR_UNSUPPORTED
+
+
+def test_nonfinite_is_reported(dns):
+    n = 16
+    U, V, W, _ = dns.tgv_fields(n)
+    U = U.copy()
+    U[3, 4, 5] = np.nan
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        eh, el, oh, ol = ctx.diagnostics_dd()
+        assert np.isnan(eh)
+        st = ctx._lib.dns_diagnostics(ctx._h, None, None, None, None)
+        assert st == dns.DNS_ERR_NONFINITE
+
+
+def test_step_before_velocity_is_an_error(dns):
+    with dns.Context(16) as ctx:
+        with pytest.raises(dns.DNSError) as e:
+            ctx.step(0.01, 0.01, 1)
+        assert e.value.status == dns.DNS_ERR_STATE
+
+
+# ---------------------------------------------------------------- CLI
+
+
+@pytest.mark.parametrize("level,T,fixture", [(5, "0.2", "refrun_tgv32_nu0.01_dt0.01_T0.2.txt"),
+                                             (6, "1", "refrun_tgv64_nu0.01_dt0.01_T1.txt")])
+def test_cli_matches_reference_run(dns, tmp_path, level, T, fixture):
+    raw = str(tmp_path / "tgv.raw")
+    dns.write_raw(raw, dns.tgv_fields(1 << level))
+    r = subprocess.run([dns.CLI_PATH, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", T],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = r.stdout.splitlines()
+    want = open(os.path.join(GOLDEN, fixture)).read().splitlines()
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        ga, wa = g.split(), w.split()
+        assert g[:10] == w[:10] and ga[:2] == wa[:2] and len(g) == len(w)
+        for x, y in zip(ga[2:], wa[2:]):
+            assert abs(float(x) - float(y)) <= E_TOL * abs(float(y))
+
+
+def test_cli_dump_matches_reference(dns, oracle_lib, tmp_path):
+    """-d writes the same .raw fields (1e-11) and byte-identical XDMF as the
+    reference main.c (run here through oracle/_ref on the same input)."""
+    n = 16
+    U, V, W = random_field(n, 21)
+    (tmp_path / "mine").mkdir()
+    (tmp_path / "ref").mkdir()
+    raw = str(tmp_path / "in.raw")
+    dns.write_raw(raw, [U, V, W, np.zeros_like(U)])
+    args = ["-d", "-i", raw, "-n", "0.02", "-s", "0.005", "-t", "0.1"]
+    r1 = subprocess.run([dns.CLI_PATH, *args], capture_output=True, text=True, cwd=tmp_path / "mine")
+    r2 = subprocess.run([oracle_lib.REF_DNS, *args], capture_output=True, text=True, cwd=tmp_path / "ref")
+    assert r1.returncode == 0 and r2.returncode == 0, r1.stderr
+    names = sorted(os.listdir(tmp_path / "ref"))
+    assert sorted(os.listdir(tmp_path / "mine")) == names
+    for name in names:
+        a = (tmp_path / "mine" / name).read_bytes()
+        b = (tmp_path / "ref" / name).read_bytes()
+        if name.endswith(".xdmf2"):
+            assert a == b
+        elif name != "00000000.raw":  # step 0: the reference's P is uninitialised
+            fa = np.frombuffer(a).reshape(4, n, n, n)
+            fb = np.frombuffer(b).reshape(4, n, n, n)
+            assert rel_l2(fa[:3], fb[:3]) <= FIELD_TOL
+            assert rel_l2(fa[3], fb[3]) <= FIELD_TOL
+        else:
+            fa = np.frombuffer(a).reshape(4, n, n, n)
+            fb = np.frombuffer(b).reshape(4, n, n, n)
+            assert rel_l2(fa[:3], fb[:3]) <= ROUND_TOL

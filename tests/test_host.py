@@ -1,0 +1,121 @@
+"""CPU tests of the host side: the C ABI exports, the CLI's argument and
+input handling (compared with the reference main.c's own behaviour), the
+step schedule and the print format.  No GPU: every CLI case here exits
+before the first CUDA call."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+
+def declared_functions():
+    hdr = open(os.path.join(ROOT, "include", "dns_b200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(dns_[a-z_0-9]+)\s*\(", hdr)))
+
+
+def test_library_exports_every_declared_symbol(dns_lib):
+    names = declared_functions()
+    assert "dns_step" in names and "dns_create" in names
+    for name in names:
+        assert hasattr(dns_lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", dns_lib._name], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (dns_\w+)", out))
+    assert set(names) <= exported
+
+
+def test_strerror_without_gpu(dns_lib):
+    import dns_b200
+
+    assert dns_lib.dns_strerror(dns_b200.DNS_OK) == b"success"
+    assert b"unsupported" in dns_lib.dns_strerror(dns_b200.DNS_ERR_UNSUPPORTED)
+
+
+CLI_CASES = [
+    [],
+    ["-x"],
+    ["-i"],
+    ["-n"],
+    ["-s"],
+    ["-t"],
+    ["-n", "0.1x"],
+    ["-t", "1", "-n", "0.01", "-s", "0.01"],
+    ["-t", "1", "-n", "0.01", "-i", "in.raw"],
+    ["-t", "1", "-s", "0.01", "-i", "in.raw"],
+    ["-n", "0.01", "-s", "0.01", "-i", "in.raw"],
+    ["-t", "0", "-n", "0.01", "-s", "0.01", "-i", "in.raw"],
+    ["-t", "1", "-n", "0.01", "-s", "0.01", "-i", "missing.raw"],
+    ["-t", "1", "-n", "0.01", "-s", "0.01", "-i", "bad.raw"],
+]
+
+
+@pytest.mark.parametrize("args", CLI_CASES, ids=[" ".join(a) or "noargs" for a in CLI_CASES])
+def test_cli_errors_match_reference(dns_lib, oracle_lib, tmp_path, args):
+    import dns_b200
+
+    (tmp_path / "bad.raw").write_bytes(b"\0" * (8 * 4 * 8 + 8))  # not 4 n^3 doubles
+    (tmp_path / "in.raw").write_bytes(b"\0" * (8 * 4 * 8))
+    mine = subprocess.run([dns_b200.CLI_PATH, *args], capture_output=True, text=True, cwd=tmp_path)
+    ref = subprocess.run([oracle_lib.REF_DNS, *args], capture_output=True, text=True, cwd=tmp_path)
+    assert mine.returncode == ref.returncode == 1
+    assert mine.stdout == ref.stdout == ""
+    assert mine.stderr == ref.stderr
+
+
+def test_cli_help_text(dns_lib, oracle_lib):
+    import dns_b200
+
+    mine = subprocess.run([dns_b200.CLI_PATH, "-h"], capture_output=True, text=True)
+    ref = subprocess.run([oracle_lib.REF_DNS, "-h"], capture_output=True, text=True)
+    assert mine.returncode == ref.returncode == 1
+    # identical usage; only the build-info line names the backend
+    assert mine.stderr.split("\nBuild Info:")[0] == ref.stderr.split("\nBuild Info:")[0]
+
+
+@pytest.mark.parametrize("T,dt,steps", [(1.0, 0.01, 100), (10.0, 0.005, 2000), (10.0, 0.0025, 4000),
+                                        (0.5, 0.0025, 200), (2.0, 0.005, 401)])
+def test_step_schedule(T, dt, steps):
+    """main.c:332-333, 421: stop when the accumulated t exceeds T."""
+    import dns_b200
+
+    sched, total = dns_b200.step_schedule(T, dt)
+    assert total == steps
+    assert sched[0] == (0, 0.0)
+    assert all(s % 10 == 0 for s, _ in sched)
+
+
+def test_format_line_matches_reference_output():
+    import dns_b200
+
+    from conftest import read_history
+
+    for name in ("ref_0128_1600.txt", "ref_0256_3000.txt", "refrun_tgv64_nu0.01_dt0.01_T1.txt"):
+        path = os.path.join(GOLDEN, name)
+        steps, ts, E, Om = read_history(path)
+        lines = open(path).read().splitlines()
+        for q in range(len(lines)):
+            assert dns_b200.format_line(int(steps[q]), float(ts[q]), E[q], Om[q]) == lines[q]
+
+
+def test_raw_roundtrip(tmp_path):
+    import dns_b200
+
+    f = dns_b200.tgv_fields(8)
+    p = str(tmp_path / "a.raw")
+    dns_b200.write_raw(p, f)
+    n, a = dns_b200.read_raw(p)
+    assert n == 8 and np.array_equal(a[0], f[0]) and np.array_equal(a[1], f[1])
+
+
+def test_product_does_not_import_oracle():
+    """The product package has no path into the oracle (no CPU fallback)."""
+    pkg = os.path.join(ROOT, "dns_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for fn in files:
+            if fn.endswith((".py", ".c", ".cu", ".cuh", ".h")):
+                text = open(os.path.join(dirpath, fn)).read()
+                assert "import oracle" not in text and "liboracle" not in text, fn
