@@ -60,7 +60,8 @@ def test_r2c_known_answer_n8(dns):
     with dns.Context(n) as ctx:
         ctx.set_velocity(x, x, x)
         uh = ctx.get_spectral()
-    assert np.abs(uh[0] - ref).max() <= 1e-12
+    # the naive DFT itself carries ~n^3 eps of rounding
+    assert np.abs(uh[0] - ref).max() <= 1e-14 * n ** 3 * np.abs(x).max()
 
 
 @pytest.mark.parametrize("n", [8, 16, 32, 64, 128])
@@ -119,13 +120,14 @@ def test_stale_velocity_quirk_is_reproduced(dns, oracle_lib):
 
 
 def test_tgv64_config_plain(dns, oracle_lib):
-    """64^3 Taylor-Green, nu = 0.01, dt = 0.01, T = 1 (100 steps): energy /
+    """64^3 Taylor-Green, nu = 0.01, dt = 0.01, T = 1 (100 steps, the t > T
+    test of main.c:332 with accumulated t stops at 100): energy /
     enstrophy every 10 steps against the reference main.c's own run
     (refrun fixture) and the oracle, final fields against the oracle."""
     n, nu, dt, T = 64, 0.01, 0.01, 1.0
     steps, ts, Eg, Og = read_history(os.path.join(GOLDEN, "refrun_tgv64_nu0.01_dt0.01_T1.txt"))
     sched, total = dns.step_schedule(T, dt)
-    assert total == 101 and [s for s, _ in sched] == list(steps)
+    assert total == 100 and [s for s, _ in sched] == list(steps)
     U, V, W, _ = dns.tgv_fields(n)
     with dns.Context(n) as ctx:
         ctx.set_velocity(U, V, W)
