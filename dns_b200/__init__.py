@@ -30,8 +30,9 @@ DNS_PREC_FP64 = 0
 DNS_FLAG_PRESSURE = 1
 
 SUPPORTED_N = (8, 16, 32, 64, 128, 256, 512)
-KERNELS_PER_STEP = 20
-PASS_NAMES = ("A:x-inverse", "B:y-inverse", "C:z-fused", "D:y-forward", "E:x-forward+update")
+KERNELS_PER_STAGE = 6
+KERNELS_PER_STEP = 4 * KERNELS_PER_STAGE
+PASS_NAMES = ("A:x-inverse", "B:y-inverse", "C:z-fused", "D:y-forward", "E1:x-forward", "E2:update")
 
 
 class DNSError(RuntimeError):

@@ -30,6 +30,9 @@ namespace {
 thread_local std::string g_last_error;
 
 enum { SLOT_SA = 0, SLOT_SB = 3, SLOT_ACC = 6, SLOT_WORK = 9, SLOT_P = 16, NSLOTS = 17 };
+// per RK stage: A x-inverse, B y-inverse, C z fused, D y-forward,
+// E1 x-forward, E2 pointwise update
+enum { KERNELS_PER_STAGE = 6 };
 
 int fail(int code, const char *what, const char *file, int line) {
   char buf[512];
@@ -96,7 +99,7 @@ struct dns_ctx {
   bool have_state = false;
   cudaGraphExec_t graph = nullptr;
   double graph_nu = 0, graph_dt = 0;
-  int kernels_per_step = 20;
+  int kernels_per_step = 4 * KERNELS_PER_STAGE;
 };
 
 namespace {
@@ -139,8 +142,8 @@ struct Ops {
   static constexpr int E = Plan<N>::E;
   static constexpr int CT = (N / E) * W;
   static constexpr size_t COL_SMEM = (size_t)(N + N * W) * sizeof(cd);
-  static constexpr size_t UPD_SMEM = (size_t)(N + 3 * N * W) * sizeof(cd);
-  static constexpr size_t Z_SMEM = (size_t)(N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(cd);
+  static constexpr size_t Z_SMEM = (size_t)(2 * N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(cd);
+  static constexpr size_t ZS_SMEM = ZC<N>::SMEM;
 
   template <class K>
   static cudaError_t allow(K kern, size_t smem) {
@@ -152,13 +155,9 @@ struct Ops {
     if ((e = allow(k_colpass<N, W, 0, true>, COL_SMEM))) return e;
     if ((e = allow(k_colpass<N, W, 1, false>, COL_SMEM))) return e;
     if ((e = allow(k_colpass<N, W, 1, true>, COL_SMEM))) return e;
-    if ((e = allow(k_xfwd_update<N, W, 0>, UPD_SMEM))) return e;
-    if ((e = allow(k_xfwd_update<N, W, 1>, UPD_SMEM))) return e;
-    if ((e = allow(k_xfwd_update<N, W, 2>, UPD_SMEM))) return e;
-    if ((e = allow(k_xfwd_update<N, W, 3>, UPD_SMEM))) return e;
-    if ((e = allow(k_zstage<N, 0>, Z_SMEM))) return e;
-    if ((e = allow(k_zstage<N, 1>, Z_SMEM))) return e;
-    if ((e = allow(k_zstage<N, 2>, Z_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 0>, ZS_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 1>, ZS_SMEM))) return e;
+    if ((e = allow(k_zstage<N, 2>, ZS_SMEM))) return e;
     if ((e = allow(k_zr2c<N>, Z_SMEM))) return e;
     if ((e = allow(k_zc2r<N>, Z_SMEM))) return e;
     return cudaSuccess;
@@ -171,8 +170,9 @@ struct Ops {
   }
 
   static dim3 zgrid(int nfields) { return dim3((N * N) / ZCfg<N>::LINES, nfields); }
+  static dim3 zsgrid() { return dim3((N * N + ZC<N>::LINES - 1) / ZC<N>::LINES); }
 
-  // kernel `k` (0..4) of RK stage `s`
+  // kernel `k` (0..KERNELS_PER_STAGE-1) of RK stage `s`
   static void stage_kernel(dns_ctx *c, int s, int k, double nu, double dt) {
     const Geo &g = c->g;
     cd *work = c->S + SLOT_WORK * g.slot;
@@ -186,15 +186,20 @@ struct Ops {
         break;
       case 2:
         if (s == 0)
-          k_zstage<N, 0><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+          k_zstage<N, 0><<<zsgrid(), ZC<N>::THREADS, ZS_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
         else if (s < 3)
-          k_zstage<N, 1><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+          k_zstage<N, 1><<<zsgrid(), ZC<N>::THREADS, ZS_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
         else
-          k_zstage<N, 2><<<zgrid(1), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
+          k_zstage<N, 2><<<zsgrid(), ZC<N>::THREADS, ZS_SMEM, c->stream>>>(work, c->stale, c->tw, g, invn3);
         break;
-      case 3: {
+      case 3:
+      case 4: {
+        // D: y forward, E1: x forward (in place on the three N slots)
         const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
-        colpass<1, true>(c, jobs_map(io, io, 3), 3);
+        if (k == 3)
+          colpass<1, true>(c, jobs_map(io, io, 3), 3);
+        else
+          colpass<0, true>(c, jobs_map(io, io, 3), 3);
         break;
       }
       default: {
@@ -208,12 +213,14 @@ struct Ops {
         sa.dt = dt;
         sa.a = RK_A[s];
         sa.b = s < 3 ? RK_B[s] : 0.0;
-        dim3 grid(g.nfp / W, N);
+        const long long npts = (long long)N * N * g.nf;
+        const int per = UPD_THREADS * UPD_PER_THREAD;
+        dim3 grid((unsigned)((npts + per - 1) / per));
         switch (s) {
-          case 0: k_xfwd_update<N, W, 0><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
-          case 1: k_xfwd_update<N, W, 1><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
-          case 2: k_xfwd_update<N, W, 2><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
-          default: k_xfwd_update<N, W, 3><<<grid, CT, UPD_SMEM, c->stream>>>(work, c->tw, g, sa); break;
+          case 0: k_update<0><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
+          case 1: k_update<1><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
+          case 2: k_update<2><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
+          default: k_update<3><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
         }
       }
     }
@@ -221,7 +228,7 @@ struct Ops {
 
   static void step(dns_ctx *c, double nu, double dt) {
     for (int s = 0; s < 4; s++)
-      for (int k = 0; k < 5; k++) stage_kernel(c, s, k, nu, dt);
+      for (int k = 0; k < KERNELS_PER_STAGE; k++) stage_kernel(c, s, k, nu, dt);
   }
 
   // forward transform of the three stale real slots into SA
@@ -532,7 +539,7 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
   for (long s = 0; s < nsteps && st == DNS_OK; s++) {
     CK(cudaEventRecord(ev[0], c->stream));
     for (int k = 0; k < K; k++) {
-      dispatch(c->n, [&](auto ops) { decltype(ops)::stage_kernel(c, k / 5, k % 5, nu, dt); });
+      dispatch(c->n, [&](auto ops) { decltype(ops)::stage_kernel(c, k / KERNELS_PER_STAGE, k % KERNELS_PER_STAGE, nu, dt); });
       CK(cudaEventRecord(ev[k + 1], c->stream));
     }
     st = check_launch(__FILE__, __LINE__);

@@ -12,8 +12,8 @@
 // backward = exp(+2 pi i jk/L), no normalisation.
 //
 // Twiddles come from a table tw[k] = exp(-2 pi i k / n), k in [0, n), of the
-// grid size n (generated on the host in long double and rounded once); a
-// length-L transform reads it with stride n/L.
+// grid size n (generated on the host in long double and rounded once),
+// regrouped per stage in shared memory (StageTw).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -130,6 +130,18 @@ template <> struct Plan<128> { static constexpr int E = 16, NS = 2, R0 = 16, R1 
 template <> struct Plan<256> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 16, R2 = 1, R3 = 1; };
 template <> struct Plan<512> { static constexpr int E = 8,  NS = 3, R0 = 8,  R1 = 8, R2 = 8, R3 = 1; };
 
+// Plans for the full-length complex FFTs of the fused z pass: E = 8 values
+// per thread keeps the three u x omega accumulators in registers.
+template <int L>
+struct ZFPlan;
+template <> struct ZFPlan<8>   { static constexpr int E = 8, NS = 1, R0 = 8, R1 = 1, R2 = 1, R3 = 1; };
+template <> struct ZFPlan<16>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 2, R2 = 1, R3 = 1; };
+template <> struct ZFPlan<32>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 4, R2 = 1, R3 = 1; };
+template <> struct ZFPlan<64>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 8, R2 = 1, R3 = 1; };
+template <> struct ZFPlan<128> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 2, R3 = 1; };
+template <> struct ZFPlan<256> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 4, R3 = 1; };
+template <> struct ZFPlan<512> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 8, R3 = 1; };
+
 // Plans for the half-length complex FFT of the z (real) axis, one warp or
 // less per line: E <= 8 keeps registers free for the fused pointwise work.
 template <int M>
@@ -142,18 +154,51 @@ template <> struct ZPlan<64>  { static constexpr int E = 4, NS = 3, R0 = 4, R1 =
 template <> struct ZPlan<128> { static constexpr int E = 4, NS = 4, R0 = 4, R1 = 4, R2 = 4, R3 = 2; };
 template <> struct ZPlan<256> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 4, R3 = 1; };
 
+// Stage twiddle tables.  Stage s >= 1 of a plan (NSV = product of the
+// earlier radices, R = its radix) needs W_{NSV*R}^{jm*r} for jm < NSV and
+// 1 <= r < R.  They are kept in shared memory as [r-1][jm], so that lanes
+// with consecutive jm read consecutive words (no bank conflicts) and lanes
+// with equal jm read the same word (broadcast).
+template <class P>
+struct StageTw {
+  static constexpr int N1 = P::R0, N2 = P::R0 * P::R1, N3 = P::R0 * P::R1 * P::R2;
+  static constexpr int O1 = 0;
+  static constexpr int O2 = O1 + (P::NS > 1 ? N1 * (P::R1 - 1) : 0);
+  static constexpr int O3 = O2 + (P::NS > 2 ? N2 * (P::R2 - 1) : 0);
+  static constexpr int SIZE = O3 + (P::NS > 3 ? N3 * (P::R3 - 1) : 0);
+};
+
+// Fill the stage tables of plan P for a line of length L from the length-n
+// table twg[k] = exp(-2 pi i k / n) (global memory).  Caller syncs.
+template <int L, class P>
+__device__ __forceinline__ void build_stage_tw(cd *st, const cd *__restrict__ twg, int n) {
+  using S = StageTw<P>;
+  for (int i = threadIdx.x; i < S::SIZE; i += blockDim.x) {
+    int nsv, R, loc;
+    if (i < S::O2) {
+      nsv = S::N1; R = P::R1; loc = i - S::O1;
+    } else if (i < S::O3) {
+      nsv = S::N2; R = P::R2; loc = i - S::O2;
+    } else {
+      nsv = S::N3; R = P::R3; loc = i - S::O3;
+    }
+    const int r = loc / nsv + 1, jm = loc % nsv;
+    st[i] = twg[(long long)jm * r * (n / (nsv * R))];
+  }
+}
+
 // One Stockham stage on the strided distribution.
 //   L: line length, E: values per thread, R: radix, NSV: product of the
 //   radices of the previous stages.  Butterfly j = t + T*q (q < E/R) reads
 //   positions j + r*L/R (= registers q + r*E/R), applies the twiddles
-//   W_{NSV*R}^{(j mod NSV)*r}, runs a radix-R DFT and sends output r to
-//   position (j/NSV)*NSV*R + (j mod NSV) + r*NSV.
+//   W_{NSV*R}^{(j mod NSV)*r} (table tws, layout [r-1][jm]), runs a radix-R
+//   DFT and sends output r to position (j/NSV)*NSV*R + (j mod NSV) + r*NSV.
 // For the last stage (NSV*R == L) the destination is register q + r*E/R,
 // so no exchange is needed.  Otherwise outputs go to xbuf via idx(pos),
 // sync() is called, and the strided distribution is read back.
 template <int L, int E, int R, int NSV, bool FWD, class Idx, class Sync>
-__device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *__restrict__ tw,
-                                      const int twstride, cd *xbuf, Idx idx, Sync sync) {
+__device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *tws, cd *xbuf, Idx idx,
+                                      Sync sync) {
   constexpr int T = L / E;
   constexpr int Q = E / R;
   constexpr bool LAST = (NSV * R == L);
@@ -165,10 +210,8 @@ __device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *__restr
     const int j = t + T * q;
     if constexpr (NSV > 1) {
       const int jm = j % NSV;
-      // twiddle index in the length-n table: jm * r * (L / (NSV*R)) * twstride
-      const int base = jm * (L / (NSV * R)) * twstride;
 #pragma unroll
-      for (int r = 1; r < R; r++) a[r] = twmul<FWD>(a[r], tw[base * r]);
+      for (int r = 1; r < R; r++) a[r] = twmul<FWD>(a[r], tws[(r - 1) * NSV + jm]);
     }
     dft<R, FWD>(a);
     if constexpr (LAST) {
@@ -188,17 +231,17 @@ __device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *__restr
   }
 }
 
-// Full line FFT of length L with plan P (P::E must equal E).
+// Full line FFT of length L with plan P (P::E must equal E); st = the
+// plan's stage twiddle tables (build_stage_tw).
 template <int L, class P, bool FWD, class Idx, class Sync>
-__device__ __forceinline__ void line_fft(cd (&v)[P::E], const int t, const cd *__restrict__ tw,
-                                         const int twstride, cd *xbuf, Idx idx, Sync sync) {
+__device__ __forceinline__ void line_fft(cd (&v)[P::E], const int t, const cd *st, cd *xbuf,
+                                         Idx idx, Sync sync) {
   constexpr int E = P::E;
-  stage<L, E, P::R0, 1, FWD>(v, t, tw, twstride, xbuf, idx, sync);
-  if constexpr (P::NS > 1) stage<L, E, P::R1, P::R0, FWD>(v, t, tw, twstride, xbuf, idx, sync);
-  if constexpr (P::NS > 2)
-    stage<L, E, P::R2, P::R0 * P::R1, FWD>(v, t, tw, twstride, xbuf, idx, sync);
-  if constexpr (P::NS > 3)
-    stage<L, E, P::R3, P::R0 * P::R1 * P::R2, FWD>(v, t, tw, twstride, xbuf, idx, sync);
+  using S = StageTw<P>;
+  stage<L, E, P::R0, 1, FWD>(v, t, st, xbuf, idx, sync);
+  if constexpr (P::NS > 1) stage<L, E, P::R1, S::N1, FWD>(v, t, st + S::O1, xbuf, idx, sync);
+  if constexpr (P::NS > 2) stage<L, E, P::R2, S::N2, FWD>(v, t, st + S::O2, xbuf, idx, sync);
+  if constexpr (P::NS > 3) stage<L, E, P::R3, S::N3, FWD>(v, t, st + S::O3, xbuf, idx, sync);
 }
 
 // signed wavenumber of index i on an n-point axis (main.c:224-230:

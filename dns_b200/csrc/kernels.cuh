@@ -63,10 +63,6 @@ struct PadIdx {
   __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> 3); }
 };
 
-__device__ __forceinline__ void load_tw(cd *tw, const cd *__restrict__ twg, int n) {
-  for (int k = threadIdx.x; k < n; k += blockDim.x) tw[k] = twg[k];
-  __syncthreads();
-}
 
 // ---------------------------------------------------------------------------
 // Column pass along x (AXIS 0) or y (AXIS 1), forward or backward.
@@ -78,9 +74,10 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
               Geo g, ColJobs jobs) {
   constexpr int E = Plan<N>::E, T = N / E;
   extern __shared__ cd smem[];
-  cd *tw = smem;
+  cd *st = smem;  // stage twiddles (<= N entries)
   cd *xb = smem + N;
-  load_tw(tw, twg, N);
+  build_stage_tw<N, Plan<N>>(st, twg, N);
+  __syncthreads();
   const int p = threadIdx.x % W, t = threadIdx.x / W;
   const int col = blockIdx.x * W + p;
   const bool ok = col < g.nf;
@@ -108,7 +105,7 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
     }
   }
   if (oslot >= 0) {
-    line_fft<N, Plan<N>, FWD>(v, t, tw, 1, xb, ColIdx<W>{p}, BlockSync{});
+    line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, BlockSync{});
     if (ok) {
       cd *dst = out + (long long)oslot * g.slot + base;
 #pragma unroll
@@ -116,7 +113,7 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
     }
   }
   if (dslot >= 0) {
-    line_fft<N, Plan<N>, FWD>(d, t, tw, 1, xb, ColIdx<W>{p}, BlockSync{});
+    line_fft<N, Plan<N>, FWD>(d, t, st, xb, ColIdx<W>{p}, BlockSync{});
     if (ok) {
       cd *dst = out + (long long)dslot * g.slot + base;
 #pragma unroll
@@ -161,7 +158,7 @@ __device__ __forceinline__ void partners(const cd (&v)[E], cd (&pp)[E], int t, i
 // The imaginary parts of X[0] and X[M] are ignored (FFTW c2r semantics).
 template <int N>
 __device__ __forceinline__ void c2r_line(cd (&v)[ZCfg<N>::E], cd xm, int t, int lane0,
-                                         const cd *tw, cd *xb) {
+                                         const cd *tw, const cd *st, cd *xb) {
   using C = ZCfg<N>;
   constexpr int E = C::E, TZ = C::TZ;
   if (t == 0) {
@@ -178,17 +175,17 @@ __device__ __forceinline__ void c2r_line(cd (&v)[ZCfg<N>::E], cd xm, int t, int 
     const cd c = cmulc(b, tw[k]);                                   // W^{-k} b
     v[e] = make_double2(a.x - c.y, a.y + c.x);                      // a + i c
   }
-  line_fft<C::M, ZPlan<C::M>, false>(v, t, tw, 2, xb, PadIdx{}, WarpSync{});
+  line_fft<C::M, ZPlan<C::M>, false>(v, t, st, xb, PadIdx{}, WarpSync{});
 }
 
 // r2c of one z line: in: z[m] = (x[2m], x[2m+1]) at m = t + TZ*e;
 // out: X[k] at k = t + TZ*e, and X[M] returned in xm (valid in lane t == 0).
 template <int N>
 __device__ __forceinline__ void r2c_line(cd (&v)[ZCfg<N>::E], cd &xm, int t, int lane0,
-                                         const cd *tw, cd *xb) {
+                                         const cd *tw, const cd *st, cd *xb) {
   using C = ZCfg<N>;
   constexpr int E = C::E, TZ = C::TZ;
-  line_fft<C::M, ZPlan<C::M>, true>(v, t, tw, 2, xb, PadIdx{}, WarpSync{});
+  line_fft<C::M, ZPlan<C::M>, true>(v, t, st, xb, PadIdx{}, WarpSync{});
   cd pp[E];
   partners<E, TZ>(v, pp, t, lane0, v[0]);
   xm = make_double2(v[0].x - v[0].y, 0.0);
@@ -236,121 +233,216 @@ __device__ __forceinline__ void ikz(const cd (&v)[ZCfg<N>::E], cd xm, cd (&o)[ZC
 
 // ---------------------------------------------------------------------------
 // Pass C: per z line, build omega, c2r u and omega, N = u x omega, r2c N.
+//
+// Each real transform pair runs as ONE complex N-point FFT ("two for one"):
+//   c2r: Y[k] = A_ext[k] + i B_ext[k] with the Hermitian extension
+//        X_ext[k] = X[k] (k <= N/2), conj(X[N-k]) (k > N/2) and the
+//        imaginary parts of X[0], X[N/2] dropped (FFTW c2r semantics, the
+//        z axis being the last, real one); Re y = a, Im y = b.
+//   r2c: Y = a + i b; X_a[k] = (Z[k] + conj Z[N-k]) / 2,
+//        X_b[k] = -i (Z[k] - conj Z[N-k]) / 2.
+// T = N/E threads per line hold E points each (ZFPlan<N>); the velocity is
+// staged in shared memory (each thread only reads back its own points), the
+// three u x omega accumulators stay in registers.
 // KIND 0: first stage, velocity from the stale real slots (main.c:344 skips
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
-// grid: N*N / LINES blocks.
 // ---------------------------------------------------------------------------
+template <int N>
+struct ZC {
+  using P = ZFPlan<N>;
+  static constexpr int E = P::E;
+  static constexpr int T = N / E;                 // threads per line
+  static constexpr int M = N / 2;
+  static constexpr int WANT = 128;
+  static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
+  static constexpr int LINES = THREADS / T;
+  static constexpr int MINB = 3;                  // blocks per SM (caps registers at 170)
+  static constexpr int PADSH = (E >= 16) ? 4 : 3;
+  static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (cd)
+  static constexpr int STASH = 5 * N;             // doubles per line: u, v, w, N_y, N_z
+  static constexpr size_t SMEM = (size_t)(N + LINES * XB) * sizeof(cd) + (size_t)LINES * STASH * 8;
+};
+
+template <int SH>
+struct PadShift {
+  __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> SH); }
+};
+
+template <bool BLOCK>
+struct LineSync {
+  __device__ __forceinline__ void operator()() const {
+    if (BLOCK) __syncthreads(); else __syncwarp();
+  }
+};
+
+// Hermitian-extended pair  Y[k] = A_ext[k] + i B_ext[k]  at k = t + T*e.
+// Loads are issued in chunks of CH positions (an empty asm with a memory
+// clobber keeps the compiler from hoisting all of them), which bounds the
+// registers held by loads in flight.
+template <int N, int CH = 4, class FA, class FB>
+__device__ __forceinline__ void ext_pair(cd (&y)[ZC<N>::E], int t, FA fa, FB fb) {
+  using C = ZC<N>;
+#pragma unroll
+  for (int e0 = 0; e0 < C::E; e0 += CH) {
+#pragma unroll
+    for (int e = e0; e < e0 + CH && e < C::E; e++) {
+      const int k = t + C::T * e;
+      const bool direct = k <= C::M;
+      const int s = direct ? k : N - k;
+      cd a = fa(s), b = fb(s);
+      if (s == 0 || s == C::M) {
+        a.y = 0.0;
+        b.y = 0.0;
+      }
+      if (!direct) {
+        a.y = -a.y;
+        b.y = -b.y;
+      }
+      y[e] = make_double2(a.x - b.y, a.y + b.x);
+    }
+    asm volatile("" ::: "memory");
+  }
+}
+
 template <int N, int KIND>
-__global__ void __launch_bounds__(ZCfg<N>::THREADS)
+__global__ void __launch_bounds__(ZC<N>::THREADS, ZC<N>::MINB)
     k_zstage(cd *__restrict__ work, double *__restrict__ stale, const cd *__restrict__ twg, Geo g,
              double invn3) {
-  using C = ZCfg<N>;
-  constexpr int E = C::E, TZ = C::TZ;
+  using C = ZC<N>;
+  constexpr int E = C::E, T = C::T, M = C::M;
   extern __shared__ cd smem[];
-  cd *tw = smem;
-  load_tw(tw, twg, N);
-  const int lid = threadIdx.x / TZ;  // line within block
-  const int t = threadIdx.x % TZ;
-  const int lane0 = (threadIdx.x & 31) - t;
+  cd *tw = smem;  // stage twiddles of ZFPlan<N> (<= N entries)
+  build_stage_tw<N, typename C::P>(tw, twg, N);
+  __syncthreads();
+  const int lid = threadIdx.x / T, t = threadIdx.x % T;
   cd *xb = smem + N + lid * C::XB;
+  double *st = (double *)(smem + N + C::LINES * C::XB) + lid * C::STASH;
+  // own points of field f: st[(f * E + e) * T + t]
+  auto SU_ = [&](int f, int e) -> double & { return st[(f * E + e) * T + t]; };
   const long long line = (long long)blockIdx.x * C::LINES + lid;
   const bool ok = line < (long long)N * N;
   const long long off = line * g.nfp;
-  const long long roff = line * N;  // real line offset
+  const cd *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
+  const cd *pW = work + SW * g.slot + off, *pDVDX = work + SDVDX * g.slot + off;
+  const cd *pDWDX = work + SDWDX * g.slot + off, *pDUDY = work + SDUDY * g.slot + off;
+  const cd *pDWDY = work + SDWDY * g.slot + off;
+  const cd zero = make_double2(0.0, 0.0);
+  auto ld = [&](const cd *p, int s) -> cd { return ok ? p[s] : zero; };
+  auto f_ox = [&](int s) -> cd {  // omega_x = dw/dy - i kz v
+    const cd a = ld(pDWDY, s), v = ld(pV, s);
+    return make_double2(a.x + s * v.y, a.y - s * v.x);
+  };
+  auto f_oy = [&](int s) -> cd {  // omega_y = i kz u - dw/dx
+    const cd u = ld(pU, s), b = ld(pDWDX, s);
+    return make_double2(-s * u.y - b.x, s * u.x - b.y);
+  };
+  auto f_oz = [&](int s) -> cd {  // omega_z = dv/dx - du/dy
+    return csub(ld(pDVDX, s), ld(pDUDY, s));
+  };
+  auto f_zero = [&](int) -> cd { return zero; };
+  const LineSync<(T > 32)> sync{};
+  const PadShift<C::PADSH> idx{};
+  const long long roff = line * N;
 
-  cd u[E], vv[E], w[E];    // real velocity, pairs (x[2m], x[2m+1]) at m = t + TZ e
-  cd oy[E], oym, ox[E], oxm;  // spectral omega_y, omega_x
-  {
-    cd a[E], am, b[E], bm;
-    // omega_y = i kz u - dw/dx
-    load_zline<N>(a, am, work + SU * g.slot + off, t, ok);
-    load_zline<N>(b, bm, work + SDWDX * g.slot + off, t, ok);
-    ikz<N>(a, am, oy, oym, t);
-#pragma unroll
-    for (int e = 0; e < E; e++) oy[e] = csub(oy[e], b[e]);
-    oym = csub(oym, bm);
-    if (KIND != 0) {
-      c2r_line<N>(a, am, t, lane0, tw, xb);
-#pragma unroll
-      for (int e = 0; e < E; e++) u[e] = cscale(a[e], invn3);
-    }
-    // omega_x = dw/dy - i kz v
-    load_zline<N>(a, am, work + SV * g.slot + off, t, ok);
-    load_zline<N>(b, bm, work + SDWDY * g.slot + off, t, ok);
-    ikz<N>(a, am, ox, oxm, t);
-#pragma unroll
-    for (int e = 0; e < E; e++) ox[e] = csub(b[e], ox[e]);
-    oxm = csub(bm, oxm);
-    if (KIND != 0) {
-      c2r_line<N>(a, am, t, lane0, tw, xb);
-#pragma unroll
-      for (int e = 0; e < E; e++) vv[e] = cscale(a[e], invn3);
-      load_zline<N>(a, am, work + SW * g.slot + off, t, ok);
-      c2r_line<N>(a, am, t, lane0, tw, xb);
-#pragma unroll
-      for (int e = 0; e < E; e++) w[e] = cscale(a[e], invn3);
-    }
-  }
+  cd y[E];
+  double nx[E], ny[E], nz[E];
   if (KIND == 0) {
-    const double *s = stale + roff;
+    // stale real velocity, own points m = t + T e
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int m = t + TZ * e;
-      u[e] = ok ? *(const double2 *)(s + 2 * m) : make_double2(0.0, 0.0);
-      vv[e] = ok ? *(const double2 *)(s + g.nreal + 2 * m) : make_double2(0.0, 0.0);
-      w[e] = ok ? *(const double2 *)(s + 2 * g.nreal + 2 * m) : make_double2(0.0, 0.0);
+      const int m = t + T * e;
+#pragma unroll
+      for (int f = 0; f < 3; f++) SU_(f, e) = ok ? stale[f * g.nreal + roff + m] : 0.0;
     }
-  }
-  if (KIND == 2 && ok) {
-    double *s = stale + roff;
+    ext_pair<N>(y, t, f_ox, f_oy);
+    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int m = t + TZ * e;
-      *(double2 *)(s + 2 * m) = u[e];
-      *(double2 *)(s + g.nreal + 2 * m) = vv[e];
-      *(double2 *)(s + 2 * g.nreal + 2 * m) = w[e];
+      const double ox = y[e].x * invn3, oy = y[e].y * invn3;
+      const double u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
+      nx[e] = -w * oy;
+      ny[e] = w * ox;
+      nz[e] = u * oy - v * ox;
     }
-  }
-  // N = u x omega  (main.c:372-377), accumulated one omega component at a time
-  cd nx[E], ny[E], nz[E];
-  c2r_line<N>(ox, oxm, t, lane0, tw, xb);
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const cd o = cscale(ox[e], invn3);
-    ny[e] = make_double2(w[e].x * o.x, w[e].y * o.y);
-    nz[e] = make_double2(-vv[e].x * o.x, -vv[e].y * o.y);
-  }
-  c2r_line<N>(oy, oym, t, lane0, tw, xb);
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const cd o = cscale(oy[e], invn3);
-    nx[e] = make_double2(-w[e].x * o.x, -w[e].y * o.y);
-    nz[e] = make_double2(nz[e].x + u[e].x * o.x, nz[e].y + u[e].y * o.y);
-  }
-  {
-    cd a[E], am, b[E], bm;
-    load_zline<N>(a, am, work + SDVDX * g.slot + off, t, ok);
-    load_zline<N>(b, bm, work + SDUDY * g.slot + off, t, ok);
-#pragma unroll
-    for (int e = 0; e < E; e++) a[e] = csub(a[e], b[e]);  // omega_z = dv/dx - du/dy
-    am = csub(am, bm);
-    c2r_line<N>(a, am, t, lane0, tw, xb);
+    ext_pair<N>(y, t, f_oz, f_zero);
+    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const cd o = cscale(a[e], invn3);
-      nx[e] = make_double2(nx[e].x + vv[e].x * o.x, nx[e].y + vv[e].y * o.y);
-      ny[e] = make_double2(ny[e].x - u[e].x * o.x, ny[e].y - u[e].y * o.y);
+      const double oz = y[e].x * invn3;
+      nx[e] += SU_(1, e) * oz;
+      ny[e] -= SU_(0, e) * oz;
+    }
+  } else {
+    // (u, v)
+    ext_pair<N>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
+    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      SU_(0, e) = y[e].x * invn3;
+      SU_(1, e) = y[e].y * invn3;
+    }
+    // (w, omega_x)
+    ext_pair<N>(y, t, [&](int s) { return ld(pW, s); }, f_ox);
+    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double w = y[e].x * invn3, ox = y[e].y * invn3;
+      SU_(2, e) = w;
+      SU_(3, e) = w * ox;            // partial N_y
+      SU_(4, e) = -SU_(1, e) * ox;   // partial N_z
+    }
+    // (omega_y, omega_z)
+    ext_pair<N>(y, t, f_oy, f_oz);
+    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double oy = y[e].x * invn3, oz = y[e].y * invn3;
+      const double u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
+      nx[e] = v * oz - w * oy;
+      ny[e] = SU_(3, e) - u * oz;
+      nz[e] = SU_(4, e) + u * oy;
+    }
+    if (KIND == 2 && ok) {
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int m = t + T * e;
+#pragma unroll
+        for (int f = 0; f < 3; f++) stale[f * g.nreal + roff + m] = SU_(f, e);
+      }
     }
   }
-  // forward z transforms of N into slots U, V, W (main.c:378-380)
-  cd xm;
-  r2c_line<N>(nx, xm, t, lane0, tw, xb);
-  store_zline<N>(nx, xm, work + SU * g.slot + off, t, ok);
-  r2c_line<N>(ny, xm, t, lane0, tw, xb);
-  store_zline<N>(ny, xm, work + SV * g.slot + off, t, ok);
-  r2c_line<N>(nz, xm, t, lane0, tw, xb);
-  store_zline<N>(nz, xm, work + SW * g.slot + off, t, ok);
+  // forward: (N_x, N_y) as one complex FFT, then N_z  (main.c:378-380)
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = make_double2(nx[e], ny[e]);
+  line_fft<N, typename C::P, true>(y, t, tw, xb, idx, sync);
+#pragma unroll
+  for (int e = 0; e < E; e++) xb[idx(t + T * e)] = y[e];
+  sync();
+  cd *oU = work + SU * g.slot + off, *oV = work + SV * g.slot + off;
+#pragma unroll
+  for (int e = 0; e <= E / 2; e++) {
+    const int k = t + T * e;
+    if (k <= M) {
+      const cd z = y[e], p = xb[idx((N - k) & (N - 1))];
+      const cd a = make_double2(0.5 * (z.x + p.x), 0.5 * (z.y - p.y));   // (Z + conj P) / 2
+      const cd d = make_double2(0.5 * (z.x - p.x), 0.5 * (z.y + p.y));   // (Z - conj P) / 2
+      if (ok) {
+        oU[k] = a;
+        oV[k] = make_double2(d.y, -d.x);  // -i d
+      }
+    }
+  }
+  sync();
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = make_double2(nz[e], 0.0);
+  line_fft<N, typename C::P, true>(y, t, tw, xb, idx, sync);
+  cd *oW = work + SW * g.slot + off;
+#pragma unroll
+  for (int e = 0; e <= E / 2; e++) {
+    const int k = t + T * e;
+    if (k <= M && ok) oW[k] = y[e];
+  }
 }
 
 // z r2c of real slots (initial transform, main.c:249-251): real slot f ->
@@ -362,11 +454,14 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
   using C = ZCfg<N>;
   constexpr int E = C::E, TZ = C::TZ;
   extern __shared__ cd smem[];
-  cd *tw = smem;
-  load_tw(tw, twg, N);
+  cd *tw = smem;       // full table exp(-2 pi i k / N): pre/post twiddles
+  cd *st = smem + N;   // stage twiddles of ZPlan<N/2>
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  __syncthreads();
   const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
   const int lane0 = (threadIdx.x & 31) - t;
-  cd *xb = smem + N + lid * C::XB;
+  cd *xb = smem + 2 * N + lid * C::XB;
   const long long line = (long long)blockIdx.x * C::LINES + lid;
   const bool ok = line < (long long)N * N;
   const double *s = real + blockIdx.y * g.nreal + line * N;
@@ -374,7 +469,7 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 #pragma unroll
   for (int e = 0; e < E; e++)
     v[e] = ok ? *(const double2 *)(s + 2 * (t + TZ * e)) : make_double2(0.0, 0.0);
-  r2c_line<N>(v, xm, t, lane0, tw, xb);
+  r2c_line<N>(v, xm, t, lane0, tw, st, xb);
   store_zline<N>(v, xm, work + blockIdx.y * g.slot + line * g.nfp, t, ok);
 }
 
@@ -386,16 +481,19 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
   using C = ZCfg<N>;
   constexpr int E = C::E, TZ = C::TZ;
   extern __shared__ cd smem[];
-  cd *tw = smem;
-  load_tw(tw, twg, N);
+  cd *tw = smem;       // full table exp(-2 pi i k / N): pre/post twiddles
+  cd *st = smem + N;   // stage twiddles of ZPlan<N/2>
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  __syncthreads();
   const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
   const int lane0 = (threadIdx.x & 31) - t;
-  cd *xb = smem + N + lid * C::XB;
+  cd *xb = smem + 2 * N + lid * C::XB;
   const long long line = (long long)blockIdx.x * C::LINES + lid;
   const bool ok = line < (long long)N * N;
   cd v[E], xm;
   load_zline<N>(v, xm, work + blockIdx.y * g.slot + line * g.nfp, t, ok);
-  c2r_line<N>(v, xm, t, lane0, tw, xb);
+  c2r_line<N>(v, xm, t, lane0, tw, st, xb);
   if (ok) {
     double *d = real + blockIdx.y * g.nreal + line * N;
 #pragma unroll
@@ -404,15 +502,16 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 }
 
 // ---------------------------------------------------------------------------
-// Pass E: x forward transform of the three N slots, then per point
-// (main.c:381-413):
+// Pass E: after the x forward transform of the three N slots (a column pass),
+// the pointwise update of main.c:381-413 on the full half spectrum:
 //   dU  = N * (mask * dt)
 //   P   = kk > 0 ? (dU kx + dV ky + dW kz) / kk : 0
 //   dU -= P kx + nu dt kk U_s          (same for V, W)
 //   ST 0:   next = u0 + b0 dU,  acc = u0 + a0 dU      (u_s == u0)
 //   ST 1,2: next = u0 + b dU,   acc += a dU
 //   ST 3:   u0   = acc + a3 dU   (the state of the next step)
-// grid: (nfp / W, n); block: (N / E) * W threads.
+// A pure streaming kernel: one thread per half-spectrum point, UPT points
+// per thread in flight.
 // ---------------------------------------------------------------------------
 struct StageArgs {
   cd *u0;      // step start state (3 slots); ST 3 writes the new state here
@@ -423,85 +522,71 @@ struct StageArgs {
   double nu, dt, a, b;
 };
 
-template <int N, int W, int ST>
-__global__ void __launch_bounds__((N / Plan<N>::E) * W)
-    k_xfwd_update(const cd *__restrict__ work, const cd *__restrict__ twg, Geo g, StageArgs sa) {
-  constexpr int E = Plan<N>::E, T = N / E;
-  extern __shared__ cd smem[];
-  cd *tw = smem;
-  cd *res = smem + N;  // [3][N][W]
-  load_tw(tw, twg, N);
-  const int p = threadIdx.x % W, t = threadIdx.x / W;
-  const int col = blockIdx.x * W + p;
-  const bool ok = col < g.nf;
-  const int j = blockIdx.y;
-  const long long base = (long long)j * g.nfp + col;
-  const long long rs = (long long)N * g.nfp;
-#pragma unroll 1
-  for (int f = 0; f < 3; f++) {
-    const cd *src = work + f * g.slot + base;
-    cd v[E];
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : make_double2(0.0, 0.0);
-    cd *r = res + f * N * W;
-    line_fft<N, Plan<N>, true>(v, t, tw, 1, r, ColIdx<W>{p}, BlockSync{});
-#pragma unroll
-    for (int e = 0; e < E; e++) r[(t + T * e) * W + p] = v[e];
+template <int ST>
+__device__ __forceinline__ void update_point(const cd *__restrict__ nl, const Geo &g, const StageArgs &sa,
+                                             long long q) {
+  const long long row = q / g.nf;
+  const int col = (int)(q - row * g.nf);
+  const int i = (int)(row / g.n), j = (int)(row - (long long)i * g.n);
+  const long long o = row * g.nfp + col;
+  const int ikx = kwave(i, g.n), iky = kwave(j, g.n);
+  const double kx = (double)ikx, ky = (double)iky, kz = (double)col;
+  const bool in = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
+                  col <= g.kcut;
+  const double md = (double)in * sa.dt;
+  cd du = cscale(nl[o], md);
+  cd dv = cscale(nl[g.slot + o], md);
+  cd dw = cscale(nl[2 * g.slot + o], md);
+  const double kk = kx * kx + ky * ky + kz * kz;
+  cd P;
+  if (kk > 0) {
+    P.x = (du.x * kx + dv.x * ky + dw.x * kz) / kk;
+    P.y = (du.y * kx + dv.y * ky + dw.y * kz) / kk;
+  } else {
+    P = make_double2(0.0, 0.0);
   }
-  if (!ok) return;
-  const double ky = (double)kwave(j, N);
-  const double kz = (double)col;
-  const bool ky_in = (j < N / 2 ? j : N - j) <= g.kcut;  // |kwave(j)|
-  const bool kz_in = col <= g.kcut;
-#pragma unroll 2
-  for (int e = 0; e < E; e++) {
-    const int row = t + T * e;
-    const int ikx = kwave(row, N);
-    const double kx = (double)ikx;
-    const bool kx_in = (ikx < 0 ? -ikx : ikx) <= g.kcut;
-    const double md = (double)(kx_in && ky_in && kz_in) * sa.dt;
-    const long long o = row * rs + base;
-    // own points only: same thread wrote r[row][p] above
-    cd du = cscale(res[(0 * N + row) * W + p], md);
-    cd dv = cscale(res[(1 * N + row) * W + p], md);
-    cd dw = cscale(res[(2 * N + row) * W + p], md);
-    const double kk = kx * kx + ky * ky + kz * kz;
-    cd P;
-    if (kk > 0) {
-      P.x = (du.x * kx + dv.x * ky + dw.x * kz) / kk;
-      P.y = (du.y * kx + dv.y * ky + dw.y * kz) / kk;
-    } else {
-      P = make_double2(0.0, 0.0);
-    }
-    const double c = sa.nu * sa.dt * kk;
-    const cd us0 = sa.us[o], us1 = sa.us[g.slot + o], us2 = sa.us[2 * g.slot + o];
-    du = make_double2(du.x - (P.x * kx + c * us0.x), du.y - (P.y * kx + c * us0.y));
-    dv = make_double2(dv.x - (P.x * ky + c * us1.x), dv.y - (P.y * ky + c * us1.y));
-    dw = make_double2(dw.x - (P.x * kz + c * us2.x), dw.y - (P.y * kz + c * us2.y));
-    if (sa.ph) sa.ph[o] = P;
-    if (ST == 0) {
-      // us == u0
-      sa.next[o] = make_double2(us0.x + sa.b * du.x, us0.y + sa.b * du.y);
-      sa.next[g.slot + o] = make_double2(us1.x + sa.b * dv.x, us1.y + sa.b * dv.y);
-      sa.next[2 * g.slot + o] = make_double2(us2.x + sa.b * dw.x, us2.y + sa.b * dw.y);
-      sa.acc[o] = make_double2(us0.x + sa.a * du.x, us0.y + sa.a * du.y);
-      sa.acc[g.slot + o] = make_double2(us1.x + sa.a * dv.x, us1.y + sa.a * dv.y);
-      sa.acc[2 * g.slot + o] = make_double2(us2.x + sa.a * dw.x, us2.y + sa.a * dw.y);
-    } else if (ST < 3) {
-      const cd z0 = sa.u0[o], z1 = sa.u0[g.slot + o], z2 = sa.u0[2 * g.slot + o];
-      const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
-      sa.next[o] = make_double2(z0.x + sa.b * du.x, z0.y + sa.b * du.y);
-      sa.next[g.slot + o] = make_double2(z1.x + sa.b * dv.x, z1.y + sa.b * dv.y);
-      sa.next[2 * g.slot + o] = make_double2(z2.x + sa.b * dw.x, z2.y + sa.b * dw.y);
-      sa.acc[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
-      sa.acc[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
-      sa.acc[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
-    } else {
-      const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
-      sa.u0[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
-      sa.u0[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
-      sa.u0[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
-    }
+  const double c = sa.nu * sa.dt * kk;
+  const cd us0 = sa.us[o], us1 = sa.us[g.slot + o], us2 = sa.us[2 * g.slot + o];
+  du = make_double2(du.x - (P.x * kx + c * us0.x), du.y - (P.y * kx + c * us0.y));
+  dv = make_double2(dv.x - (P.x * ky + c * us1.x), dv.y - (P.y * ky + c * us1.y));
+  dw = make_double2(dw.x - (P.x * kz + c * us2.x), dw.y - (P.y * kz + c * us2.y));
+  if (sa.ph) sa.ph[o] = P;
+  if (ST == 0) {  // us == u0
+    sa.next[o] = make_double2(us0.x + sa.b * du.x, us0.y + sa.b * du.y);
+    sa.next[g.slot + o] = make_double2(us1.x + sa.b * dv.x, us1.y + sa.b * dv.y);
+    sa.next[2 * g.slot + o] = make_double2(us2.x + sa.b * dw.x, us2.y + sa.b * dw.y);
+    sa.acc[o] = make_double2(us0.x + sa.a * du.x, us0.y + sa.a * du.y);
+    sa.acc[g.slot + o] = make_double2(us1.x + sa.a * dv.x, us1.y + sa.a * dv.y);
+    sa.acc[2 * g.slot + o] = make_double2(us2.x + sa.a * dw.x, us2.y + sa.a * dw.y);
+  } else if (ST < 3) {
+    const cd z0 = sa.u0[o], z1 = sa.u0[g.slot + o], z2 = sa.u0[2 * g.slot + o];
+    const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
+    sa.next[o] = make_double2(z0.x + sa.b * du.x, z0.y + sa.b * du.y);
+    sa.next[g.slot + o] = make_double2(z1.x + sa.b * dv.x, z1.y + sa.b * dv.y);
+    sa.next[2 * g.slot + o] = make_double2(z2.x + sa.b * dw.x, z2.y + sa.b * dw.y);
+    sa.acc[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
+    sa.acc[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
+    sa.acc[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
+  } else {
+    const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
+    sa.u0[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
+    sa.u0[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
+    sa.u0[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
+  }
+}
+
+constexpr int UPD_THREADS = 256;
+constexpr int UPD_PER_THREAD = 2;
+
+template <int ST>
+__global__ void __launch_bounds__(UPD_THREADS)
+    k_update(const cd *__restrict__ nl, Geo g, StageArgs sa) {
+  const long long npts = (long long)g.n * g.n * g.nf;
+  const long long q0 = (long long)blockIdx.x * UPD_THREADS * UPD_PER_THREAD + threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < UPD_PER_THREAD; u++) {
+    const long long q = q0 + (long long)u * UPD_THREADS;
+    if (q < npts) update_point<ST>(nl, g, sa, q);
   }
 }
 
