@@ -73,6 +73,7 @@ _SIGS = {
     "dns_get_stream": (_P, [_P]),
     "dns_synchronize": (ctypes.c_int, [_P]),
     "dns_time_kernels": (ctypes.c_int, [_P, _D, _D, ctypes.c_long, ctypes.POINTER(_D)]),
+    "dns_diagnostics_noalloc": (ctypes.c_int, [ctypes.c_long, _P, _P, _P]),
 }
 
 

@@ -80,6 +80,10 @@ void sincos2pi(long k, long n, double *c, double *s) {
 
 }  // namespace
 
+namespace dnsb {
+void set_last_error(const char *msg) { g_last_error = msg; }
+}  // namespace dnsb
+
 struct dns_ctx {
   long n = 0;
   int precision = 0;

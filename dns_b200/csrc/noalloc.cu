@@ -1,0 +1,121 @@
+// noalloc.cu -- energy/enstrophy of a caller-owned spectral velocity with no
+// device allocation at all (dns_diagnostics_noalloc in include/dns_b200.h).
+//
+// Who needs it: callers that may not call cudaMalloc at the point where they
+// want the diagnostics -- code recording work into a CUDA graph with a
+// capture mode that forbids allocation, frameworks whose memory pool already
+// holds the device memory they are allowed to use, and tight monitoring loops
+// that cannot afford the implicit synchronisation an allocation can bring.
+// They hand in device pointers for the input and the four output doubles and
+// get the same double-double sums as dns_diagnostics.
+//
+// The reduction needs scratch for its per-block partial sums.  Here that
+// scratch is a fixed file-scope device array, NOALLOC_MAX_PARTIALS entries of
+// 32 bytes (263 KB), present on every GPU that loads the library until the
+// process exits.  Each block reduces a fixed chunk of NOALLOC_CHUNK points,
+// so the array bounds the problem size: n^2 (n/2+1) <= NOALLOC_MAX_PARTIALS *
+// NOALLOC_CHUNK = 67,371,008 points, which is exactly the n = 512 grid;
+// anything larger is rejected before anything is launched.
+#include "dns_b200.h"
+#include "kernels.cuh"
+
+#include <mutex>
+#include <stdio.h>
+
+using namespace dnsb;
+
+namespace dnsb {
+void set_last_error(const char *msg);  // dns_api.cu: text for dns_last_error()
+}
+
+namespace {
+
+constexpr int NOALLOC_THREADS = 256;
+constexpr int NOALLOC_PER_THREAD = 32;
+constexpr long long NOALLOC_CHUNK = (long long)NOALLOC_THREADS * NOALLOC_PER_THREAD;  // 8192
+constexpr int NOALLOC_MAX_PARTIALS = 8224;  // = ceil(512^2 * 257 / NOALLOC_CHUNK)
+
+// Shared by every call on a device.  Every block of a call writes its own
+// entry before the final block reads it, so nothing has to start at zero; two
+// calls that overlap on the GPU (different streams, no ordering) race on it.
+__device__ __align__(256) double4 g_noalloc_partials[NOALLOC_MAX_PARTIALS];
+
+// device address of g_noalloc_partials, looked up once per device
+constexpr int MAX_DEVICES = 64;
+double4 *g_partials_addr[MAX_DEVICES] = {};
+std::mutex g_setup_mutex;
+
+// Same terms and double-double arithmetic as k_diag, but each block reduces
+// the fixed chunk [blockIdx.x * NOALLOC_CHUNK, +NOALLOC_CHUNK) of points of an
+// unpadded [3][n][n][n/2+1] array.
+__global__ void __launch_bounds__(NOALLOC_THREADS)
+    k_diag_chunk(const cd *__restrict__ u, int n, long long npts, double4 *__restrict__ partial) {
+  const int nf = n / 2 + 1;
+  DD e{0.0, 0.0}, o{0.0, 0.0};
+  const long long base = (long long)blockIdx.x * NOALLOC_CHUNK;
+#pragma unroll 4
+  for (int i = 0; i < NOALLOC_PER_THREAD; i++) {
+    const long long q = base + threadIdx.x + (long long)i * NOALLOC_THREADS;
+    if (q < npts) {
+      const long long row = q / nf;
+      const int k = (int)(q - row * nf);
+      const int ii = (int)(row / n), jj = (int)(row % n);
+      const double s = __dadd_rn(__dadd_rn(cabs2_rn(u[q]), cabs2_rn(u[npts + q])),
+                                 cabs2_rn(u[2 * npts + q]));
+      const double kx = kwave(ii, n), ky = kwave(jj, n), kz = k;
+      const double kk =
+          __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+      e = dd_add_d(e, s);
+      o = dd_add_d(o, __dmul_rn(kk, s));
+    }
+  }
+  dd_block_reduce<NOALLOC_THREADS>(e, o, partial + blockIdx.x);
+}
+
+int noalloc_fail(int code, const char *msg) {
+  dnsb::set_last_error(msg);
+  return code;
+}
+
+}  // namespace
+
+extern "C" int dns_diagnostics_noalloc(long n, const double *uvw_hat, double *out, void *stream) {
+  if (n < 8 || n > 512 || (n & (n - 1)) != 0)
+    return noalloc_fail(DNS_ERR_UNSUPPORTED,
+                        "dns_diagnostics_noalloc: n must be a power of two in [8, 512]");
+  const long long npts = (long long)n * n * (n / 2 + 1);
+  const long long nblocks = (npts + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
+  if (nblocks > NOALLOC_MAX_PARTIALS)
+    return noalloc_fail(DNS_ERR_UNSUPPORTED,
+                        "dns_diagnostics_noalloc: input larger than the fixed scratch "
+                        "(n^2 (n/2+1) must be <= 67371008 points, n <= 512)");
+  if (!uvw_hat || !out) return noalloc_fail(DNS_ERR_ARG, "dns_diagnostics_noalloc: NULL pointer");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= MAX_DEVICES)
+    return noalloc_fail(DNS_ERR_UNSUPPORTED, "dns_diagnostics_noalloc: device index too large");
+  double4 *partials = nullptr;
+  {
+    // set-up, once per device, with that device current: the host-side name
+    // g_noalloc_partials is only a stand-in, the kernel needs the device
+    // address.  This first call on a device also loads the module, so it
+    // should happen before any stream capture.
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_partials_addr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+      if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+      g_partials_addr[dev] = (double4 *)p;
+    }
+    partials = g_partials_addr[dev];
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  k_diag_chunk<<<(unsigned)nblocks, NOALLOC_THREADS, 0, s>>>((const cd *)uvw_hat, (int)n, npts,
+                                                            partials);
+  k_diag_final<NOALLOC_THREADS><<<1, NOALLOC_THREADS, 0, s>>>(partials, (int)nblocks,
+                                                              (double4 *)out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+  return DNS_OK;
+}

@@ -124,6 +124,31 @@ int dns_synchronize(dns_ctx *ctx);
  * nsteps. */
 int dns_time_kernels(dns_ctx *ctx, double nu, double dt, long nsteps, double *ms);
 
+/* Energy and enstrophy of a spectral velocity held in caller-owned device
+ * memory, allocating nothing.  No counterpart in the reference (main.c has
+ * no library interface); this is an addition for callers that may not call
+ * cudaMalloc where they need the diagnostics: work being recorded into a CUDA
+ * graph, frameworks whose memory pool owns the device memory, monitoring
+ * loops that must not trigger the synchronisation an allocation can cause.
+ *   n       grid size, power of two in [8, 512]
+ *   uvw_hat device pointer, [3][n][n][n/2+1] complex float64 (the layout of
+ *           dns_get_spectral), unnormalised like FFTW's r2c
+ *   out     device pointer to 4 doubles: e_hi, e_lo, om_hi, om_lo, the same
+ *           double-double sums dns_diagnostics returns (scale by
+ *           invn3 * invn3 as main.c:265-266 does)
+ *   stream  a cudaStream_t (NULL: the legacy default stream); the call only
+ *           queues work, the caller synchronises before reading out
+ * Scratch is a fixed 263 KB device array inside the library (every GPU that
+ * loads the library holds it until exit), sized for the n = 512 grid: larger
+ * inputs (more than 67,371,008 half-spectrum points) are rejected with
+ * DNS_ERR_UNSUPPORTED, as is any n outside the range.  The first call on a device looks up that array's device
+ * address and loads the kernels, so make it before any stream capture.
+ * Every call shares the array: calls that can overlap on the GPU (different
+ * streams without ordering, or different host threads on one device) race;
+ * serialise them.  Nothing in it has to start at zero (each call overwrites
+ * every entry it reads). */
+int dns_diagnostics_noalloc(long n, const double *uvw_hat, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
