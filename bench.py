@@ -302,6 +302,41 @@ def main() -> int:
         pass
     step_bytes = sum(map(sum, pb))
 
+    # -- mixed precision (FP32 fields/FFTs, FP64 reductions/coefficients) --
+    E64, O64 = ctx.diagnostics()  # after warmup + timed + 3 kernel-timing steps
+    done64 = args.warmup + args.steps + 3
+    with dns_b200.Context(n, dns_b200.DNS_PREC_MIXED) as cm:
+        sm = torch.cuda.ExternalStream(cm.stream)
+        cm.set_velocity(U, V, W)
+        cm.step(NU, DT, args.warmup)
+        cm.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(sm)
+        cm.step(NU, DT, args.steps)
+        m1.record(sm)
+        m1.synchronize()
+        mixed_ms = m0.elapsed_time(m1)
+        cm.step(NU, DT, done64 - args.warmup - args.steps)
+        E32, O32 = cm.diagnostics()
+        mkms = cm.time_kernels(NU, DT, 2).reshape(4, K)
+    if pg is not None:
+        t = torch.tensor([mixed_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        mixed_ms = float(t.item())
+    mixed_sps = args.steps / (mixed_ms / 1000.0)
+    mixed = {
+        "value": mixed_sps * world, "unit": "steps/s", "ms_per_step": mixed_ms / args.steps,
+        "speedup_vs_fp64": mixed_sps / steps_per_s,
+        "energy_rel_err_vs_fp64": float(abs(E32 - E64) / E64),
+        "enstrophy_rel_err_vs_fp64": float(abs(O32 - O64) / O64),
+        "compared_after_steps": done64,
+        "step_hbm_frac_of_model_roofline": step_bytes_model(n) / 2 * mixed_sps / (peak * 1e9),
+        "kernel_ms": {dns_b200.PASS_NAMES[p]: [float(mkms[s, p]) for s in range(4)] for p in range(K)},
+    }
+
     # -- end to end through the C ABI with host buffers --
     pinned = [torch.from_numpy(a.reshape(-1)).pin_memory() for a in (U, V, W)]
     outs = [torch.empty(n ** 3, dtype=torch.float64).pin_memory() for _ in range(3)]
@@ -381,6 +416,7 @@ def main() -> int:
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "wall_s": wall},
             "gpu_launches": dns_b200.KERNELS_PER_STEP * args.steps,
+            "mixed": mixed,
             "clocks": clk,
             "cpu_baseline": cpu,
         }

@@ -27,6 +27,7 @@ DNS_ERR_NOMEM = 4
 DNS_ERR_NONFINITE = 5
 DNS_ERR_STATE = 6
 DNS_PREC_FP64 = 0
+DNS_PREC_MIXED = 1
 DNS_FLAG_PRESSURE = 1
 
 SUPPORTED_N = (8, 16, 32, 64, 128, 256, 512)

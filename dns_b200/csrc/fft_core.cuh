@@ -21,26 +21,63 @@
 
 namespace dnsb {
 
+// Complex types: double2 (FP64 path) and float2 (FP32 storage of the mixed
+// path).  Every routine below is a template on the complex type C.
+template <class R>
+struct Cx;
+template <>
+struct Cx<double> {
+  using T = double2;
+};
+template <>
+struct Cx<float> {
+  using T = float2;
+};
+template <class R>
+using cx = typename Cx<R>::T;
+template <class C>
+using sc = decltype(C::x);  // scalar of a complex type
+
 typedef double2 cd;
 
-__device__ __forceinline__ cd cadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ cd csub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ cd cscale(cd a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ cd cconj(cd a) { return make_double2(a.x, -a.y); }
+template <class C>
+__device__ __forceinline__ C cmk(sc<C> a, sc<C> b) {
+  C r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <class C>
+__device__ __forceinline__ C czero() {
+  return cmk<C>(sc<C>(0), sc<C>(0));
+}
+template <class C>
+__device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <class C>
+__device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+template <class C>
+__device__ __forceinline__ C cscale(C a, sc<C> s) { return cmk<C>(a.x * s, a.y * s); }
 // a * b
-__device__ __forceinline__ cd cmul(cd a, cd b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <class C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // a * conj(b)
-__device__ __forceinline__ cd cmulc(cd a, cd b) {
-  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+template <class C>
+__device__ __forceinline__ C cmulc(C a, C b) {
+  return cmk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
-// i * a
-__device__ __forceinline__ cd cmul_i(cd a) { return make_double2(-a.y, a.x); }
 // multiply by the twiddle w (forward table entry) in the given direction
-template <bool FWD>
-__device__ __forceinline__ cd twmul(cd a, cd w) {
+template <bool FWD, class C>
+__device__ __forceinline__ C twmul(C a, C w) {
   return FWD ? cmul(a, w) : cmulc(a, w);
+}
+// widen / narrow between the two complex types
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+template <class C>
+__device__ __forceinline__ C from_d(double2 a) {
+  return cmk<C>((sc<C>)a.x, (sc<C>)a.y);
 }
 
 // cos(2 pi m / 16) and sin(2 pi m / 16) for m in [0, 4]
@@ -52,29 +89,31 @@ __host__ __device__ constexpr double c16(int m) {
                   : 0.0;
 }
 
-// a * exp(-/+ 2 pi i m / 16) with exact handling of the trivial factors
-template <int M, bool FWD>
-__device__ __forceinline__ cd w16(cd a) {
+// a * exp(-/+ 2 pi i m / 16) with exact handling of the trivial factors; the
+// constants are rounded once to the scalar type from the double literals
+template <int M, bool FWD, class C>
+__device__ __forceinline__ C w16(C a) {
+  using S = sc<C>;
   constexpr int m = M & 15;
   if constexpr (m == 0) {
     return a;
   } else if constexpr (m == 8) {
-    return make_double2(-a.x, -a.y);
+    return cmk<C>(-a.x, -a.y);
   } else if constexpr (m == 4) {  // exp(-i pi/2) = -i
-    return FWD ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+    return FWD ? cmk<C>(a.y, -a.x) : cmk<C>(-a.y, a.x);
   } else if constexpr (m == 12) {  // exp(-3 i pi/2) = +i
-    return FWD ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+    return FWD ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
   } else {
     // cos/sin of 2 pi m / 16 via quadrant symmetry
     constexpr int q = m / 4, r = m % 4;
     constexpr double c0 = c16(r), s0 = c16(4 - r);
-    constexpr double c = q == 0 ? c0 : q == 1 ? -s0 : q == 2 ? -c0 : s0;
-    constexpr double s = q == 0 ? s0 : q == 1 ? c0 : q == 2 ? -s0 : -c0;
+    constexpr S c = (S)(q == 0 ? c0 : q == 1 ? -s0 : q == 2 ? -c0 : s0);
+    constexpr S s = (S)(q == 0 ? s0 : q == 1 ? c0 : q == 2 ? -s0 : -c0);
     // forward multiplies by (c - i s), backward by (c + i s)
     if constexpr (FWD)
-      return make_double2(a.x * c + a.y * s, a.y * c - a.x * s);
+      return cmk<C>(a.x * c + a.y * s, a.y * c - a.x * s);
     else
-      return make_double2(a.x * c - a.y * s, a.y * c + a.x * s);
+      return cmk<C>(a.x * c - a.y * s, a.y * c + a.x * s);
   }
 }
 
@@ -90,16 +129,16 @@ __device__ __forceinline__ void static_for(F &&f) {
 
 // In-register DFT of size R (1, 2, 4, 8, 16), natural order in and out
 // (recursive radix-2 decimation in time).
-template <int R, bool FWD>
-__device__ __forceinline__ void dft(cd (&a)[R]) {
+template <int R, bool FWD, class C>
+__device__ __forceinline__ void dft(C (&a)[R]) {
   if constexpr (R == 1) {
     return;
   } else if constexpr (R == 2) {
-    cd t = a[1];
+    C t = a[1];
     a[1] = csub(a[0], t);
     a[0] = cadd(a[0], t);
   } else {
-    cd e[R / 2], o[R / 2];
+    C e[R / 2], o[R / 2];
 #pragma unroll
     for (int k = 0; k < R / 2; k++) {
       e[k] = a[2 * k];
@@ -109,7 +148,7 @@ __device__ __forceinline__ void dft(cd (&a)[R]) {
     dft<R / 2, FWD>(o);
     static_for<0, R / 2>([&](auto K) {
       constexpr int k = decltype(K)::value;
-      cd t = w16<k * (16 / R), FWD>(o[k]);
+      C t = w16<k * (16 / R), FWD>(o[k]);
       a[k] = cadd(e[k], t);
       a[k + R / 2] = csub(e[k], t);
     });
@@ -170,8 +209,8 @@ struct StageTw {
 
 // Fill the stage tables of plan P for a line of length L from the length-n
 // table twg[k] = exp(-2 pi i k / n) (global memory).  Caller syncs.
-template <int L, class P>
-__device__ __forceinline__ void build_stage_tw(cd *st, const cd *__restrict__ twg, int n) {
+template <int L, class P, class C>
+__device__ __forceinline__ void build_stage_tw(C *st, const C *__restrict__ twg, int n) {
   using S = StageTw<P>;
   for (int i = threadIdx.x; i < S::SIZE; i += blockDim.x) {
     int nsv, R, loc;
@@ -196,15 +235,15 @@ __device__ __forceinline__ void build_stage_tw(cd *st, const cd *__restrict__ tw
 // For the last stage (NSV*R == L) the destination is register q + r*E/R,
 // so no exchange is needed.  Otherwise outputs go to xbuf via idx(pos),
 // sync() is called, and the strided distribution is read back.
-template <int L, int E, int R, int NSV, bool FWD, class Idx, class Sync>
-__device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *tws, cd *xbuf, Idx idx,
+template <int L, int E, int R, int NSV, bool FWD, class C, class Idx, class Sync>
+__device__ __forceinline__ void stage(C (&v)[E], const int t, const C *tws, C *xbuf, Idx idx,
                                       Sync sync) {
   constexpr int T = L / E;
   constexpr int Q = E / R;
   constexpr bool LAST = (NSV * R == L);
 #pragma unroll
   for (int q = 0; q < Q; q++) {
-    cd a[R];
+    C a[R];
 #pragma unroll
     for (int r = 0; r < R; r++) a[r] = v[q + r * Q];
     const int j = t + T * q;
@@ -233,8 +272,8 @@ __device__ __forceinline__ void stage(cd (&v)[E], const int t, const cd *tws, cd
 
 // Full line FFT of length L with plan P (P::E must equal E); st = the
 // plan's stage twiddle tables (build_stage_tw).
-template <int L, class P, bool FWD, class Idx, class Sync>
-__device__ __forceinline__ void line_fft(cd (&v)[P::E], const int t, const cd *st, cd *xbuf,
+template <int L, class P, bool FWD, class C, class Idx, class Sync>
+__device__ __forceinline__ void line_fft(C (&v)[P::E], const int t, const C *st, C *xbuf,
                                          Idx idx, Sync sync) {
   constexpr int E = P::E;
   using S = StageTw<P>;

@@ -3,26 +3,32 @@
 // forward transform (main.c:249-251), the dump transforms (main.c:270-279)
 // and the energy/enstrophy reduction (main.c:257-266).
 //
+// Every kernel is a template on the storage scalar R: double for the FP64
+// path, float for the mixed path (FP32 fields and FFTs; the reductions and
+// the pointwise update arithmetic stay FP64).
+//
 // HBM layout (one "slot" = one complex field on the half spectrum):
 //   spectral slot  [i = kx index][j = ky index][k = kz index], k fastest,
-//                  row pitch nfp = nf rounded up to 8 (nf = n/2 + 1), so that
-//                  every 8-column tile row starts on a 128-byte boundary;
-//                  the padding columns are never read or written.
+//                  row pitch nfp = nf rounded up to the column tile width W
+//                  (nf = n/2 + 1; W * sizeof(complex) = 128 bytes), so every
+//                  tile row starts on a 128-byte boundary; the padding
+//                  columns are never read or written.
 //   real slot      [x][y][z], z fastest (the .raw layout of main.c:180-185).
 // The same slot shape holds partially transformed data: after the x pass the
 // first index is x instead of kx, after the y pass the second is y.
 //
-// One RK stage = five passes over HBM:
-//   A  x backward   state (3) -> u,v,w and d/dx of v,w          (per field)
-//   B  y backward   5 slots   -> u,v,w, dv/dx, dw/dx, du/dy, dw/dy (per field)
-//   C  z pass       per z line: vorticity from the 7 slots, 6 c2r, u x omega
-//                   in registers, 3 r2c; never touches real space in HBM
-//                   except for the stale velocity of stage 0 / stage 3
-//   D  y forward    3 slots, in place
-//   E  x forward    + 2/3 mask, projection, viscous term and RK4 updates
+// One RK stage = six kernels:
+//   A   x backward  state (3) -> u,v,w and d/dx of v,w            (per field)
+//   B   y backward  5 slots -> u,v,w, dv/dx, dw/dx, du/dy, dw/dy    (per field)
+//   C   z pass      per z line: vorticity from the 7 slots, u and omega to
+//                   real space, N = u x omega, N back to z spectral; real
+//                   space touches HBM only for the stale velocity
+//   D   y forward   3 slots, in place
+//   E1  x forward   3 slots, in place
+//   E2  update      2/3 mask, projection, viscous term, RK4 updates
 // The vorticity is assembled from spectral derivatives taken on the axis a
-// pass owns (x in A, y in B, z in C), so passes A, B and D work on one field
-// per tile and need no cross-field staging.
+// pass owns (x in A, y in B, z in C), so A, B, D and E1 work on one field per
+// tile and need no cross-field staging.
 #pragma once
 #include "fft_core.cuh"
 
@@ -47,6 +53,12 @@ struct ColJobs {
   int der_slot[8];   // -1: no derivative output
 };
 
+// column tile width: 128-byte tile rows
+template <class R>
+struct ColW {
+  static constexpr int W = 128 / (int)sizeof(cx<R>);
+};
+
 template <int W>
 struct ColIdx {
   int p;
@@ -58,24 +70,32 @@ struct BlockSync {
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
-// per-line exchange buffer with one pad element per 8 to spread banks
-struct PadIdx {
-  __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> 3); }
+// per-line exchange buffer with one pad element per 2^SH to spread banks
+template <int SH>
+struct PadShift {
+  __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> SH); }
 };
-
+template <bool BLOCK>
+struct LineSync {
+  __device__ __forceinline__ void operator()() const {
+    if (BLOCK) __syncthreads(); else __syncwarp();
+  }
+};
 
 // ---------------------------------------------------------------------------
 // Column pass along x (AXIS 0) or y (AXIS 1), forward or backward.
 // grid: (nfp / W, n, njobs); block: (N / E) * W threads.
 // ---------------------------------------------------------------------------
-template <int N, int W, int AXIS, bool FWD>
-__global__ void __launch_bounds__((N / Plan<N>::E) * W)
-    k_colpass(const cd *__restrict__ in, cd *__restrict__ out, const cd *__restrict__ twg,
-              Geo g, ColJobs jobs) {
+template <class R, int N, int AXIS, bool FWD>
+__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R>::W)
+    k_colpass(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
+              const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
+  using C = cx<R>;
+  constexpr int W = ColW<R>::W;
   constexpr int E = Plan<N>::E, T = N / E;
-  extern __shared__ cd smem[];
-  cd *st = smem;  // stage twiddles (<= N entries)
-  cd *xb = smem + N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *st = (C *)smem_raw;  // stage twiddles (<= N entries)
+  C *xb = st + N;
   build_stage_tw<N, Plan<N>>(st, twg, N);
   __syncthreads();
   const int p = threadIdx.x % W, t = threadIdx.x / W;
@@ -91,23 +111,23 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
     base = (long long)fixed * N * g.nfp + col;
     rs = g.nfp;
   }
-  const cd *src = in + (long long)jobs.in_slot[job] * g.slot + base;
-  cd v[E];
+  const C *src = in + (long long)jobs.in_slot[job] * g.slot + base;
+  C v[E];
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : make_double2(0.0, 0.0);
+  for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : czero<C>();
   const int oslot = jobs.out_slot[job], dslot = jobs.der_slot[job];
-  cd d[E];
+  C d[E];
   if (dslot >= 0) {
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const double k = (double)kwave(t + T * e, N);
-      d[e] = make_double2(-k * v[e].y, k * v[e].x);  // i k f
+      const R k = (R)kwave(t + T * e, N);
+      d[e] = cmk<C>(-k * v[e].y, k * v[e].x);  // i k f
     }
   }
   if (oslot >= 0) {
     line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, BlockSync{});
     if (ok) {
-      cd *dst = out + (long long)oslot * g.slot + base;
+      C *dst = out + (long long)oslot * g.slot + base;
 #pragma unroll
       for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = v[e];
     }
@@ -115,7 +135,7 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
   if (dslot >= 0) {
     line_fft<N, Plan<N>, FWD>(d, t, st, xb, ColIdx<W>{p}, BlockSync{});
     if (ok) {
-      cd *dst = out + (long long)dslot * g.slot + base;
+      C *dst = out + (long long)dslot * g.slot + base;
 #pragma unroll
       for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = d[e];
     }
@@ -123,7 +143,8 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * W)
 }
 
 // ---------------------------------------------------------------------------
-// z lines: TZ = M / E threads per line (M = N/2), 32 / TZ lines per warp.
+// Real transforms of single z lines (initial r2c, dump c2r) through a
+// half-length complex FFT: TZ = M / E threads per line (M = N/2).
 // ---------------------------------------------------------------------------
 template <int N>
 struct ZCfg {
@@ -139,13 +160,12 @@ struct ZCfg {
 // position M - k for every k = t + TZ*e held by this thread.  For t > 0 it
 // sits in lane (TZ - t) of the same line, register E-1-e; for t == 0 it is
 // this thread's register E-e, or `m_val` (position M) for e == 0.
-template <int E, int TZ>
-__device__ __forceinline__ void partners(const cd (&v)[E], cd (&pp)[E], int t, int lane0,
-                                         cd m_val) {
+template <int E, int TZ, class C>
+__device__ __forceinline__ void partners(const C (&v)[E], C (&pp)[E], int t, int lane0, C m_val) {
   const int src = lane0 + ((TZ - t) & (TZ - 1));
 #pragma unroll
   for (int e = 0; e < E; e++) {
-    cd s;
+    C s;
     s.x = __shfl_sync(0xffffffffu, v[E - 1 - e].x, src);
     s.y = __shfl_sync(0xffffffffu, v[E - 1 - e].y, src);
     if (t == 0) s = (e == 0) ? m_val : v[(E - e) % E];
@@ -156,79 +176,120 @@ __device__ __forceinline__ void partners(const cd (&v)[E], cd (&pp)[E], int t, i
 // c2r of one z line: in: X[k] at k = t + TZ*e, X[M] in xm (lane t == 0);
 // out: z[m] = (x[2m], x[2m+1]) at m = t + TZ*e, unnormalised like FFTW.
 // The imaginary parts of X[0] and X[M] are ignored (FFTW c2r semantics).
-template <int N>
-__device__ __forceinline__ void c2r_line(cd (&v)[ZCfg<N>::E], cd xm, int t, int lane0,
-                                         const cd *tw, const cd *st, cd *xb) {
-  using C = ZCfg<N>;
-  constexpr int E = C::E, TZ = C::TZ;
+template <int N, class C>
+__device__ __forceinline__ void c2r_line(C (&v)[ZCfg<N>::E], C xm, int t, int lane0, const C *tw,
+                                         const C *st, C *xb) {
+  using Z = ZCfg<N>;
+  constexpr int E = Z::E, TZ = Z::TZ;
   if (t == 0) {
-    v[0].y = 0.0;
-    xm.y = 0.0;
+    v[0].y = 0;
+    xm.y = 0;
   }
-  cd pp[E];
+  C pp[E];
   partners<E, TZ>(v, pp, t, lane0, xm);
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const int k = t + TZ * e;
-    const cd a = make_double2(v[e].x + pp[e].x, v[e].y - pp[e].y);  // X + conj P
-    const cd b = make_double2(v[e].x - pp[e].x, v[e].y + pp[e].y);  // X - conj P
-    const cd c = cmulc(b, tw[k]);                                   // W^{-k} b
-    v[e] = make_double2(a.x - c.y, a.y + c.x);                      // a + i c
+    const C a = cmk<C>(v[e].x + pp[e].x, v[e].y - pp[e].y);  // X + conj P
+    const C b = cmk<C>(v[e].x - pp[e].x, v[e].y + pp[e].y);  // X - conj P
+    const C c = cmulc(b, tw[k]);                             // W^{-k} b
+    v[e] = cmk<C>(a.x - c.y, a.y + c.x);                     // a + i c
   }
-  line_fft<C::M, ZPlan<C::M>, false>(v, t, st, xb, PadIdx{}, WarpSync{});
+  line_fft<Z::M, ZPlan<Z::M>, false>(v, t, st, xb, PadShift<3>{}, WarpSync{});
 }
 
 // r2c of one z line: in: z[m] = (x[2m], x[2m+1]) at m = t + TZ*e;
 // out: X[k] at k = t + TZ*e, and X[M] returned in xm (valid in lane t == 0).
-template <int N>
-__device__ __forceinline__ void r2c_line(cd (&v)[ZCfg<N>::E], cd &xm, int t, int lane0,
-                                         const cd *tw, const cd *st, cd *xb) {
-  using C = ZCfg<N>;
-  constexpr int E = C::E, TZ = C::TZ;
-  line_fft<C::M, ZPlan<C::M>, true>(v, t, st, xb, PadIdx{}, WarpSync{});
-  cd pp[E];
+template <int N, class C>
+__device__ __forceinline__ void r2c_line(C (&v)[ZCfg<N>::E], C &xm, int t, int lane0, const C *tw,
+                                         const C *st, C *xb) {
+  using Z = ZCfg<N>;
+  using S = sc<C>;
+  constexpr int E = Z::E, TZ = Z::TZ;
+  line_fft<Z::M, ZPlan<Z::M>, true>(v, t, st, xb, PadShift<3>{}, WarpSync{});
+  C pp[E];
   partners<E, TZ>(v, pp, t, lane0, v[0]);
-  xm = make_double2(v[0].x - v[0].y, 0.0);
+  xm = cmk<C>(v[0].x - v[0].y, S(0));
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const int k = t + TZ * e;
-    const cd ev = make_double2(0.5 * (v[e].x + pp[e].x), 0.5 * (v[e].y - pp[e].y));
-    const cd dv = make_double2(0.5 * (v[e].x - pp[e].x), 0.5 * (v[e].y + pp[e].y));
-    const cd q = cmul(tw[k], dv);
-    v[e] = make_double2(ev.x + q.y, ev.y - q.x);  // ev - i q
+    const C ev = cmk<C>(S(0.5) * (v[e].x + pp[e].x), S(0.5) * (v[e].y - pp[e].y));
+    const C dv = cmk<C>(S(0.5) * (v[e].x - pp[e].x), S(0.5) * (v[e].y + pp[e].y));
+    const C q = cmul(tw[k], dv);
+    v[e] = cmk<C>(ev.x + q.y, ev.y - q.x);  // ev - i q
   }
 }
 
-template <int N>
-__device__ __forceinline__ void load_zline(cd (&v)[ZCfg<N>::E], cd &xm, const cd *__restrict__ src,
-                                           int t, bool ok) {
-  using C = ZCfg<N>;
+// z r2c of real slots (initial transform, main.c:249-251): real slot f ->
+// work slot f.  grid: (N*N / LINES, nfields)
+template <class R, int N>
+__global__ void __launch_bounds__(ZCfg<N>::THREADS)
+    k_zr2c(const R *__restrict__ real, cx<R> *__restrict__ work, const cx<R> *__restrict__ twg,
+           Geo g) {
+  using C = cx<R>;
+  using Z = ZCfg<N>;
+  constexpr int E = Z::E, TZ = Z::TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = (C *)smem_raw;  // full table exp(-2 pi i k / N): pre/post twiddles
+  C *st = tw + N;         // stage twiddles of ZPlan<N/2>
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  __syncthreads();
+  const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
+  const int lane0 = (threadIdx.x & 31) - t;
+  C *xb = tw + 2 * N + lid * Z::XB;
+  const long long line = (long long)blockIdx.x * Z::LINES + lid;
+  const bool ok = line < (long long)N * N;
+  const R *s = real + blockIdx.y * g.nreal + line * N;
+  C v[E], xm;
 #pragma unroll
-  for (int e = 0; e < C::E; e++) v[e] = ok ? src[t + C::TZ * e] : make_double2(0.0, 0.0);
-  xm = (ok && t == 0) ? src[C::M] : make_double2(0.0, 0.0);
-}
-template <int N>
-__device__ __forceinline__ void store_zline(const cd (&v)[ZCfg<N>::E], cd xm, cd *__restrict__ dst,
-                                            int t, bool ok) {
-  using C = ZCfg<N>;
-  if (!ok) return;
+  for (int e = 0; e < E; e++) {
+    const int m = t + TZ * e;
+    v[e] = ok ? cmk<C>(s[2 * m], s[2 * m + 1]) : czero<C>();
+  }
+  r2c_line<N>(v, xm, t, lane0, tw, st, xb);
+  if (ok) {
+    C *d = work + blockIdx.y * g.slot + line * g.nfp;
 #pragma unroll
-  for (int e = 0; e < C::E; e++) dst[t + C::TZ * e] = v[e];
-  if (t == 0) dst[C::M] = xm;
+    for (int e = 0; e < E; e++) d[t + TZ * e] = v[e];
+    if (t == 0) d[Z::M] = xm;
+  }
 }
 
-// i*kz*X for the line positions held by this thread
-template <int N>
-__device__ __forceinline__ void ikz(const cd (&v)[ZCfg<N>::E], cd xm, cd (&o)[ZCfg<N>::E], cd &om,
-                                    int t) {
-  using C = ZCfg<N>;
+// z c2r of work slots into float64 real slots scaled by `scale` (dump,
+// main.c:274-277; fields handed to the host are always float64)
+template <class R, int N>
+__global__ void __launch_bounds__(ZCfg<N>::THREADS)
+    k_zc2r(const cx<R> *__restrict__ work, double *__restrict__ real,
+           const cx<R> *__restrict__ twg, Geo g, double scale) {
+  using C = cx<R>;
+  using Z = ZCfg<N>;
+  constexpr int E = Z::E, TZ = Z::TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = (C *)smem_raw;
+  C *st = tw + N;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  __syncthreads();
+  const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
+  const int lane0 = (threadIdx.x & 31) - t;
+  C *xb = tw + 2 * N + lid * Z::XB;
+  const long long line = (long long)blockIdx.x * Z::LINES + lid;
+  const bool ok = line < (long long)N * N;
+  const C *src = work + blockIdx.y * g.slot + line * g.nfp;
+  C v[E];
 #pragma unroll
-  for (int e = 0; e < C::E; e++) {
-    const double k = (double)(t + C::TZ * e);
-    o[e] = make_double2(-k * v[e].y, k * v[e].x);
+  for (int e = 0; e < E; e++) v[e] = ok ? src[t + TZ * e] : czero<C>();
+  C xm = (ok && t == 0) ? src[Z::M] : czero<C>();
+  c2r_line<N>(v, xm, t, lane0, tw, st, xb);
+  if (ok) {
+    double *d = real + blockIdx.y * g.nreal + line * N;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int m = t + TZ * e;
+      *(double2 *)(d + 2 * m) = make_double2((double)v[e].x * scale, (double)v[e].y * scale);
+    }
   }
-  const double k = (double)C::M;  // kz[n/2] = +n/2 (main.c:228)
-  om = make_double2(-k * xm.y, k * xm.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -241,16 +302,25 @@ __device__ __forceinline__ void ikz(const cd (&v)[ZCfg<N>::E], cd xm, cd (&o)[ZC
 //        z axis being the last, real one); Re y = a, Im y = b.
 //   r2c: Y = a + i b; X_a[k] = (Z[k] + conj Z[N-k]) / 2,
 //        X_b[k] = -i (Z[k] - conj Z[N-k]) / 2.
-// T = N/E threads per line hold E points each (ZFPlan<N>); the velocity is
-// staged in shared memory (each thread only reads back its own points), the
-// three u x omega accumulators stay in registers.
+// T = N/E threads per line hold E points each; the velocity and two of the
+// u x omega partial sums are staged in shared memory (each thread only reads
+// back its own points).
 // KIND 0: first stage, velocity from the stale real slots (main.c:344 skips
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
 // ---------------------------------------------------------------------------
+template <class R, int N>
+struct ZPlanFor {
+  using P = ZFPlan<N>;  // FP64: 8 values per thread (registers)
+};
 template <int N>
+struct ZPlanFor<float, N> {
+  using P = Plan<N>;    // FP32: up to 16 values per thread, fewer exchanges
+};
+
+template <class R, int N>
 struct ZC {
-  using P = ZFPlan<N>;
+  using P = typename ZPlanFor<R, N>::P;
   static constexpr int E = P::E;
   static constexpr int T = N / E;                 // threads per line
   static constexpr int M = N / 2;
@@ -259,146 +329,135 @@ struct ZC {
   static constexpr int LINES = THREADS / T;
   static constexpr int MINB = 3;                  // blocks per SM (caps registers at 170)
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
-  static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (cd)
-  static constexpr int STASH = 5 * N;             // doubles per line: u, v, w, N_y, N_z
-  static constexpr size_t SMEM = (size_t)(N + LINES * XB) * sizeof(cd) + (size_t)LINES * STASH * 8;
-};
-
-template <int SH>
-struct PadShift {
-  __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> SH); }
-};
-
-template <bool BLOCK>
-struct LineSync {
-  __device__ __forceinline__ void operator()() const {
-    if (BLOCK) __syncthreads(); else __syncwarp();
-  }
+  static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
+  static constexpr int STASH = 5 * N;             // scalars per line: u, v, w, N_y, N_z
+  static constexpr size_t SMEM =
+      (size_t)(N + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
 };
 
 // Hermitian-extended pair  Y[k] = A_ext[k] + i B_ext[k]  at k = t + T*e.
 // Loads are issued in chunks of CH positions (an empty asm with a memory
 // clobber keeps the compiler from hoisting all of them), which bounds the
 // registers held by loads in flight.
-template <int N, int CH = 4, class FA, class FB>
-__device__ __forceinline__ void ext_pair(cd (&y)[ZC<N>::E], int t, FA fa, FB fb) {
-  using C = ZC<N>;
+template <class R, int N, int CH = 4, class C, class FA, class FB>
+__device__ __forceinline__ void ext_pair(C (&y)[ZC<R, N>::E], int t, FA fa, FB fb) {
+  using Z = ZC<R, N>;
 #pragma unroll
-  for (int e0 = 0; e0 < C::E; e0 += CH) {
+  for (int e0 = 0; e0 < Z::E; e0 += CH) {
 #pragma unroll
-    for (int e = e0; e < e0 + CH && e < C::E; e++) {
-      const int k = t + C::T * e;
-      const bool direct = k <= C::M;
+    for (int e = e0; e < e0 + CH && e < Z::E; e++) {
+      const int k = t + Z::T * e;
+      const bool direct = k <= Z::M;
       const int s = direct ? k : N - k;
-      cd a = fa(s), b = fb(s);
-      if (s == 0 || s == C::M) {
-        a.y = 0.0;
-        b.y = 0.0;
+      C a = fa(s), b = fb(s);
+      if (s == 0 || s == Z::M) {
+        a.y = 0;
+        b.y = 0;
       }
       if (!direct) {
         a.y = -a.y;
         b.y = -b.y;
       }
-      y[e] = make_double2(a.x - b.y, a.y + b.x);
+      y[e] = cmk<C>(a.x - b.y, a.y + b.x);
     }
     asm volatile("" ::: "memory");
   }
 }
 
-template <int N, int KIND>
-__global__ void __launch_bounds__(ZC<N>::THREADS, ZC<N>::MINB)
-    k_zstage(cd *__restrict__ work, double *__restrict__ stale, const cd *__restrict__ twg, Geo g,
-             double invn3) {
-  using C = ZC<N>;
-  constexpr int E = C::E, T = C::T, M = C::M;
-  extern __shared__ cd smem[];
-  cd *tw = smem;  // stage twiddles of ZFPlan<N> (<= N entries)
-  build_stage_tw<N, typename C::P>(tw, twg, N);
+template <class R, int N, int KIND>
+__global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
+    k_zstage(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg, Geo g,
+             R invn3) {
+  using C = cx<R>;
+  using Z = ZC<R, N>;
+  constexpr int E = Z::E, T = Z::T, M = Z::M;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = (C *)smem_raw;  // stage twiddles of the z plan (<= N entries)
+  build_stage_tw<N, typename Z::P>(tw, twg, N);
   __syncthreads();
   const int lid = threadIdx.x / T, t = threadIdx.x % T;
-  cd *xb = smem + N + lid * C::XB;
-  double *st = (double *)(smem + N + C::LINES * C::XB) + lid * C::STASH;
-  // own points of field f: st[(f * E + e) * T + t]
-  auto SU_ = [&](int f, int e) -> double & { return st[(f * E + e) * T + t]; };
-  const long long line = (long long)blockIdx.x * C::LINES + lid;
+  C *xb = tw + N + lid * Z::XB;
+  R *st = (R *)(tw + N + Z::LINES * Z::XB) + lid * Z::STASH;
+  // own points of staged field f: st[(f * E + e) * T + t]
+  auto SU_ = [&](int f, int e) -> R & { return st[(f * E + e) * T + t]; };
+  const long long line = (long long)blockIdx.x * Z::LINES + lid;
   const bool ok = line < (long long)N * N;
   const long long off = line * g.nfp;
-  const cd *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
-  const cd *pW = work + SW * g.slot + off, *pDVDX = work + SDVDX * g.slot + off;
-  const cd *pDWDX = work + SDWDX * g.slot + off, *pDUDY = work + SDUDY * g.slot + off;
-  const cd *pDWDY = work + SDWDY * g.slot + off;
-  const cd zero = make_double2(0.0, 0.0);
-  auto ld = [&](const cd *p, int s) -> cd { return ok ? p[s] : zero; };
-  auto f_ox = [&](int s) -> cd {  // omega_x = dw/dy - i kz v
-    const cd a = ld(pDWDY, s), v = ld(pV, s);
-    return make_double2(a.x + s * v.y, a.y - s * v.x);
+  const C *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
+  const C *pW = work + SW * g.slot + off, *pDVDX = work + SDVDX * g.slot + off;
+  const C *pDWDX = work + SDWDX * g.slot + off, *pDUDY = work + SDUDY * g.slot + off;
+  const C *pDWDY = work + SDWDY * g.slot + off;
+  auto ld = [&](const C *p, int s) -> C { return ok ? p[s] : czero<C>(); };
+  auto f_ox = [&](int s) -> C {  // omega_x = dw/dy - i kz v
+    const C a = ld(pDWDY, s), v = ld(pV, s);
+    return cmk<C>(a.x + (R)s * v.y, a.y - (R)s * v.x);
   };
-  auto f_oy = [&](int s) -> cd {  // omega_y = i kz u - dw/dx
-    const cd u = ld(pU, s), b = ld(pDWDX, s);
-    return make_double2(-s * u.y - b.x, s * u.x - b.y);
+  auto f_oy = [&](int s) -> C {  // omega_y = i kz u - dw/dx
+    const C u = ld(pU, s), b = ld(pDWDX, s);
+    return cmk<C>(-(R)s * u.y - b.x, (R)s * u.x - b.y);
   };
-  auto f_oz = [&](int s) -> cd {  // omega_z = dv/dx - du/dy
+  auto f_oz = [&](int s) -> C {  // omega_z = dv/dx - du/dy
     return csub(ld(pDVDX, s), ld(pDUDY, s));
   };
-  auto f_zero = [&](int) -> cd { return zero; };
+  auto f_zero = [&](int) -> C { return czero<C>(); };
   const LineSync<(T > 32)> sync{};
-  const PadShift<C::PADSH> idx{};
+  const PadShift<Z::PADSH> idx{};
   const long long roff = line * N;
 
-  cd y[E];
-  double nx[E], ny[E], nz[E];
+  C y[E];
+  R nx[E], ny[E], nz[E];
   if (KIND == 0) {
     // stale real velocity, own points m = t + T e
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int m = t + T * e;
 #pragma unroll
-      for (int f = 0; f < 3; f++) SU_(f, e) = ok ? stale[f * g.nreal + roff + m] : 0.0;
+      for (int f = 0; f < 3; f++) SU_(f, e) = ok ? stale[f * g.nreal + roff + m] : R(0);
     }
-    ext_pair<N>(y, t, f_ox, f_oy);
-    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+    ext_pair<R, N>(y, t, f_ox, f_oy);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const double ox = y[e].x * invn3, oy = y[e].y * invn3;
-      const double u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
+      const R ox = y[e].x * invn3, oy = y[e].y * invn3;
+      const R u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
       nx[e] = -w * oy;
       ny[e] = w * ox;
       nz[e] = u * oy - v * ox;
     }
-    ext_pair<N>(y, t, f_oz, f_zero);
-    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+    ext_pair<R, N>(y, t, f_oz, f_zero);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const double oz = y[e].x * invn3;
+      const R oz = y[e].x * invn3;
       nx[e] += SU_(1, e) * oz;
       ny[e] -= SU_(0, e) * oz;
     }
   } else {
     // (u, v)
-    ext_pair<N>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
-    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+    ext_pair<R, N>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
       SU_(0, e) = y[e].x * invn3;
       SU_(1, e) = y[e].y * invn3;
     }
     // (w, omega_x)
-    ext_pair<N>(y, t, [&](int s) { return ld(pW, s); }, f_ox);
-    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+    ext_pair<R, N>(y, t, [&](int s) { return ld(pW, s); }, f_ox);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const double w = y[e].x * invn3, ox = y[e].y * invn3;
+      const R w = y[e].x * invn3, ox = y[e].y * invn3;
       SU_(2, e) = w;
       SU_(3, e) = w * ox;            // partial N_y
       SU_(4, e) = -SU_(1, e) * ox;   // partial N_z
     }
     // (omega_y, omega_z)
-    ext_pair<N>(y, t, f_oy, f_oz);
-    line_fft<N, typename C::P, false>(y, t, tw, xb, idx, sync);
+    ext_pair<R, N>(y, t, f_oy, f_oz);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const double oy = y[e].x * invn3, oz = y[e].y * invn3;
-      const double u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
+      const R oy = y[e].x * invn3, oz = y[e].y * invn3;
+      const R u = SU_(0, e), v = SU_(1, e), w = SU_(2, e);
       nx[e] = v * oz - w * oy;
       ny[e] = SU_(3, e) - u * oz;
       nz[e] = SU_(4, e) + u * oy;
@@ -414,30 +473,30 @@ __global__ void __launch_bounds__(ZC<N>::THREADS, ZC<N>::MINB)
   }
   // forward: (N_x, N_y) as one complex FFT, then N_z  (main.c:378-380)
 #pragma unroll
-  for (int e = 0; e < E; e++) y[e] = make_double2(nx[e], ny[e]);
-  line_fft<N, typename C::P, true>(y, t, tw, xb, idx, sync);
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
+  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
 #pragma unroll
   for (int e = 0; e < E; e++) xb[idx(t + T * e)] = y[e];
   sync();
-  cd *oU = work + SU * g.slot + off, *oV = work + SV * g.slot + off;
+  C *oU = work + SU * g.slot + off, *oV = work + SV * g.slot + off;
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
     if (k <= M) {
-      const cd z = y[e], p = xb[idx((N - k) & (N - 1))];
-      const cd a = make_double2(0.5 * (z.x + p.x), 0.5 * (z.y - p.y));   // (Z + conj P) / 2
-      const cd d = make_double2(0.5 * (z.x - p.x), 0.5 * (z.y + p.y));   // (Z - conj P) / 2
+      const C z = y[e], p = xb[idx((N - k) & (N - 1))];
+      const C a = cmk<C>(R(0.5) * (z.x + p.x), R(0.5) * (z.y - p.y));  // (Z + conj P) / 2
+      const C d = cmk<C>(R(0.5) * (z.x - p.x), R(0.5) * (z.y + p.y));  // (Z - conj P) / 2
       if (ok) {
         oU[k] = a;
-        oV[k] = make_double2(d.y, -d.x);  // -i d
+        oV[k] = cmk<C>(d.y, -d.x);  // -i d
       }
     }
   }
   sync();
 #pragma unroll
-  for (int e = 0; e < E; e++) y[e] = make_double2(nz[e], 0.0);
-  line_fft<N, typename C::P, true>(y, t, tw, xb, idx, sync);
-  cd *oW = work + SW * g.slot + off;
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nz[e], R(0));
+  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
+  C *oW = work + SW * g.slot + off;
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
@@ -445,86 +504,32 @@ __global__ void __launch_bounds__(ZC<N>::THREADS, ZC<N>::MINB)
   }
 }
 
-// z r2c of real slots (initial transform, main.c:249-251): real slot f ->
-// work slot f.  grid: (N*N / LINES, nfields)
-template <int N>
-__global__ void __launch_bounds__(ZCfg<N>::THREADS)
-    k_zr2c(const double *__restrict__ real, cd *__restrict__ work, const cd *__restrict__ twg,
-           Geo g) {
-  using C = ZCfg<N>;
-  constexpr int E = C::E, TZ = C::TZ;
-  extern __shared__ cd smem[];
-  cd *tw = smem;       // full table exp(-2 pi i k / N): pre/post twiddles
-  cd *st = smem + N;   // stage twiddles of ZPlan<N/2>
-  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
-  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
-  __syncthreads();
-  const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
-  const int lane0 = (threadIdx.x & 31) - t;
-  cd *xb = smem + 2 * N + lid * C::XB;
-  const long long line = (long long)blockIdx.x * C::LINES + lid;
-  const bool ok = line < (long long)N * N;
-  const double *s = real + blockIdx.y * g.nreal + line * N;
-  cd v[E], xm;
-#pragma unroll
-  for (int e = 0; e < E; e++)
-    v[e] = ok ? *(const double2 *)(s + 2 * (t + TZ * e)) : make_double2(0.0, 0.0);
-  r2c_line<N>(v, xm, t, lane0, tw, st, xb);
-  store_zline<N>(v, xm, work + blockIdx.y * g.slot + line * g.nfp, t, ok);
-}
-
-// z c2r of work slots into real slots scaled by `scale` (dump, main.c:274-277)
-template <int N>
-__global__ void __launch_bounds__(ZCfg<N>::THREADS)
-    k_zc2r(const cd *__restrict__ work, double *__restrict__ real, const cd *__restrict__ twg,
-           Geo g, double scale) {
-  using C = ZCfg<N>;
-  constexpr int E = C::E, TZ = C::TZ;
-  extern __shared__ cd smem[];
-  cd *tw = smem;       // full table exp(-2 pi i k / N): pre/post twiddles
-  cd *st = smem + N;   // stage twiddles of ZPlan<N/2>
-  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
-  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
-  __syncthreads();
-  const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
-  const int lane0 = (threadIdx.x & 31) - t;
-  cd *xb = smem + 2 * N + lid * C::XB;
-  const long long line = (long long)blockIdx.x * C::LINES + lid;
-  const bool ok = line < (long long)N * N;
-  cd v[E], xm;
-  load_zline<N>(v, xm, work + blockIdx.y * g.slot + line * g.nfp, t, ok);
-  c2r_line<N>(v, xm, t, lane0, tw, st, xb);
-  if (ok) {
-    double *d = real + blockIdx.y * g.nreal + line * N;
-#pragma unroll
-    for (int e = 0; e < E; e++) *(double2 *)(d + 2 * (t + TZ * e)) = cscale(v[e], scale);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// Pass E: after the x forward transform of the three N slots (a column pass),
-// the pointwise update of main.c:381-413 on the full half spectrum:
+// E2: after the x forward transform of the three N slots (E1), the pointwise
+// update of main.c:381-413 on the full half spectrum:
 //   dU  = N * (mask * dt)
 //   P   = kk > 0 ? (dU kx + dV ky + dW kz) / kk : 0
 //   dU -= P kx + nu dt kk U_s          (same for V, W)
 //   ST 0:   next = u0 + b0 dU,  acc = u0 + a0 dU      (u_s == u0)
 //   ST 1,2: next = u0 + b dU,   acc += a dU
 //   ST 3:   u0   = acc + a3 dU   (the state of the next step)
-// A pure streaming kernel: one thread per half-spectrum point, UPT points
-// per thread in flight.
+// A pure streaming kernel, one thread per half-spectrum point.  The
+// arithmetic is FP64 for both storage types (the FP32 path rounds on store).
 // ---------------------------------------------------------------------------
+template <class R>
 struct StageArgs {
-  cd *u0;      // step start state (3 slots); ST 3 writes the new state here
-  cd *us;      // stage input (3 slots)
-  cd *acc;     // RK accumulator (3 slots)
-  cd *next;    // next stage input (3 slots)
-  cd *ph;      // pressure slot or nullptr
+  cx<R> *u0;    // step start state (3 slots); ST 3 writes the new state here
+  cx<R> *us;    // stage input (3 slots)
+  cx<R> *acc;   // RK accumulator (3 slots)
+  cx<R> *next;  // next stage input (3 slots)
+  cx<R> *ph;    // pressure slot or nullptr
   double nu, dt, a, b;
 };
 
-template <int ST>
-__device__ __forceinline__ void update_point(const cd *__restrict__ nl, const Geo &g, const StageArgs &sa,
-                                             long long q) {
+template <class R, int ST>
+__device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const Geo &g,
+                                             const StageArgs<R> &sa, long long q) {
+  using C = cx<R>;
   const long long row = q / g.nf;
   const int col = (int)(q - row * g.nf);
   const int i = (int)(row / g.n), j = (int)(row - (long long)i * g.n);
@@ -534,11 +539,11 @@ __device__ __forceinline__ void update_point(const cd *__restrict__ nl, const Ge
   const bool in = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
                   col <= g.kcut;
   const double md = (double)in * sa.dt;
-  cd du = cscale(nl[o], md);
-  cd dv = cscale(nl[g.slot + o], md);
-  cd dw = cscale(nl[2 * g.slot + o], md);
+  double2 du = cscale(to_d(nl[o]), md);
+  double2 dv = cscale(to_d(nl[g.slot + o]), md);
+  double2 dw = cscale(to_d(nl[2 * g.slot + o]), md);
   const double kk = kx * kx + ky * ky + kz * kz;
-  cd P;
+  double2 P;
   if (kk > 0) {
     P.x = (du.x * kx + dv.x * ky + dw.x * kz) / kk;
     P.y = (du.y * kx + dv.y * ky + dw.y * kz) / kk;
@@ -546,47 +551,54 @@ __device__ __forceinline__ void update_point(const cd *__restrict__ nl, const Ge
     P = make_double2(0.0, 0.0);
   }
   const double c = sa.nu * sa.dt * kk;
-  const cd us0 = sa.us[o], us1 = sa.us[g.slot + o], us2 = sa.us[2 * g.slot + o];
+  const double2 us0 = to_d(sa.us[o]), us1 = to_d(sa.us[g.slot + o]),
+                us2 = to_d(sa.us[2 * g.slot + o]);
   du = make_double2(du.x - (P.x * kx + c * us0.x), du.y - (P.y * kx + c * us0.y));
   dv = make_double2(dv.x - (P.x * ky + c * us1.x), dv.y - (P.y * ky + c * us1.y));
   dw = make_double2(dw.x - (P.x * kz + c * us2.x), dw.y - (P.y * kz + c * us2.y));
-  if (sa.ph) sa.ph[o] = P;
+  if (sa.ph) sa.ph[o] = from_d<C>(P);
+  auto axpy = [](double2 x, double s, double2 y) {
+    return make_double2(x.x + s * y.x, x.y + s * y.y);
+  };
   if (ST == 0) {  // us == u0
-    sa.next[o] = make_double2(us0.x + sa.b * du.x, us0.y + sa.b * du.y);
-    sa.next[g.slot + o] = make_double2(us1.x + sa.b * dv.x, us1.y + sa.b * dv.y);
-    sa.next[2 * g.slot + o] = make_double2(us2.x + sa.b * dw.x, us2.y + sa.b * dw.y);
-    sa.acc[o] = make_double2(us0.x + sa.a * du.x, us0.y + sa.a * du.y);
-    sa.acc[g.slot + o] = make_double2(us1.x + sa.a * dv.x, us1.y + sa.a * dv.y);
-    sa.acc[2 * g.slot + o] = make_double2(us2.x + sa.a * dw.x, us2.y + sa.a * dw.y);
+    sa.next[o] = from_d<C>(axpy(us0, sa.b, du));
+    sa.next[g.slot + o] = from_d<C>(axpy(us1, sa.b, dv));
+    sa.next[2 * g.slot + o] = from_d<C>(axpy(us2, sa.b, dw));
+    sa.acc[o] = from_d<C>(axpy(us0, sa.a, du));
+    sa.acc[g.slot + o] = from_d<C>(axpy(us1, sa.a, dv));
+    sa.acc[2 * g.slot + o] = from_d<C>(axpy(us2, sa.a, dw));
   } else if (ST < 3) {
-    const cd z0 = sa.u0[o], z1 = sa.u0[g.slot + o], z2 = sa.u0[2 * g.slot + o];
-    const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
-    sa.next[o] = make_double2(z0.x + sa.b * du.x, z0.y + sa.b * du.y);
-    sa.next[g.slot + o] = make_double2(z1.x + sa.b * dv.x, z1.y + sa.b * dv.y);
-    sa.next[2 * g.slot + o] = make_double2(z2.x + sa.b * dw.x, z2.y + sa.b * dw.y);
-    sa.acc[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
-    sa.acc[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
-    sa.acc[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
+    const double2 z0 = to_d(sa.u0[o]), z1 = to_d(sa.u0[g.slot + o]),
+                  z2 = to_d(sa.u0[2 * g.slot + o]);
+    const double2 a0 = to_d(sa.acc[o]), a1 = to_d(sa.acc[g.slot + o]),
+                  a2 = to_d(sa.acc[2 * g.slot + o]);
+    sa.next[o] = from_d<C>(axpy(z0, sa.b, du));
+    sa.next[g.slot + o] = from_d<C>(axpy(z1, sa.b, dv));
+    sa.next[2 * g.slot + o] = from_d<C>(axpy(z2, sa.b, dw));
+    sa.acc[o] = from_d<C>(axpy(a0, sa.a, du));
+    sa.acc[g.slot + o] = from_d<C>(axpy(a1, sa.a, dv));
+    sa.acc[2 * g.slot + o] = from_d<C>(axpy(a2, sa.a, dw));
   } else {
-    const cd a0 = sa.acc[o], a1 = sa.acc[g.slot + o], a2 = sa.acc[2 * g.slot + o];
-    sa.u0[o] = make_double2(a0.x + sa.a * du.x, a0.y + sa.a * du.y);
-    sa.u0[g.slot + o] = make_double2(a1.x + sa.a * dv.x, a1.y + sa.a * dv.y);
-    sa.u0[2 * g.slot + o] = make_double2(a2.x + sa.a * dw.x, a2.y + sa.a * dw.y);
+    const double2 a0 = to_d(sa.acc[o]), a1 = to_d(sa.acc[g.slot + o]),
+                  a2 = to_d(sa.acc[2 * g.slot + o]);
+    sa.u0[o] = from_d<C>(axpy(a0, sa.a, du));
+    sa.u0[g.slot + o] = from_d<C>(axpy(a1, sa.a, dv));
+    sa.u0[2 * g.slot + o] = from_d<C>(axpy(a2, sa.a, dw));
   }
 }
 
 constexpr int UPD_THREADS = 256;
 constexpr int UPD_PER_THREAD = 2;
 
-template <int ST>
+template <class R, int ST>
 __global__ void __launch_bounds__(UPD_THREADS)
-    k_update(const cd *__restrict__ nl, Geo g, StageArgs sa) {
+    k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
   const long long npts = (long long)g.n * g.n * g.nf;
   const long long q0 = (long long)blockIdx.x * UPD_THREADS * UPD_PER_THREAD + threadIdx.x;
 #pragma unroll
   for (int u = 0; u < UPD_PER_THREAD; u++) {
     const long long q = q0 + (long long)u * UPD_THREADS;
-    if (q < npts) update_point<ST>(nl, g, sa, q);
+    if (q < npts) update_point<R, ST>(nl, g, sa, q);
   }
 }
 
@@ -595,6 +607,7 @@ __global__ void __launch_bounds__(UPD_THREADS)
 //   e = |U|^2 + |V|^2 + |W|^2   and   kk * e,
 // each term rounded like the reference's double expression (no FMA), summed
 // in double-double (error-free TwoSum), block partials then one final block.
+// FP32 storage is widened to FP64 first.
 // ---------------------------------------------------------------------------
 struct DD {
   double hi, lo;
@@ -617,7 +630,7 @@ __device__ __forceinline__ DD dd_add(DD a, DD b) {
 __device__ __forceinline__ DD dd_shfl_down(DD a, int d) {
   return DD{__shfl_down_sync(0xffffffffu, a.hi, d), __shfl_down_sync(0xffffffffu, a.lo, d)};
 }
-__device__ __forceinline__ double cabs2_rn(cd z) {
+__device__ __forceinline__ double cabs2_rn(double2 z) {
   return __dadd_rn(__dmul_rn(z.x, z.x), __dmul_rn(z.y, z.y));
 }
 
@@ -647,9 +660,9 @@ __device__ __forceinline__ void dd_block_reduce(DD &e, DD &o, double4 *out) {
   }
 }
 
-template <int BS>
+template <int BS, class C>
 __global__ void __launch_bounds__(BS)
-    k_diag(const cd *__restrict__ u, Geo g, double4 *__restrict__ partial) {
+    k_diag(const C *__restrict__ u, Geo g, double4 *__restrict__ partial) {
   DD e{0.0, 0.0}, o{0.0, 0.0};
   const int n = g.n;
   const long long npts = (long long)n * n * g.nf;
@@ -659,8 +672,8 @@ __global__ void __launch_bounds__(BS)
     const int k = (int)(q - row * g.nf);
     const int i = (int)(row / n), j = (int)(row % n);
     const long long l = row * g.nfp + k;
-    const double s = __dadd_rn(__dadd_rn(cabs2_rn(u[l]), cabs2_rn(u[g.slot + l])),
-                               cabs2_rn(u[2 * g.slot + l]));
+    const double s = __dadd_rn(__dadd_rn(cabs2_rn(to_d(u[l])), cabs2_rn(to_d(u[g.slot + l]))),
+                               cabs2_rn(to_d(u[2 * g.slot + l])));
     const double kx = kwave(i, n), ky = kwave(j, n), kz = k;
     const double kk = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
     e = dd_add_d(e, s);
@@ -679,6 +692,34 @@ __global__ void __launch_bounds__(BS) k_diag_final(const double4 *__restrict__ p
     o = dd_add(o, DD{v.z, v.w});
   }
   dd_block_reduce<BS>(e, o, out);
+}
+
+// ---------------------------------------------------------------------------
+// Precision conversions for the FP32 path (host data is always float64).
+// ---------------------------------------------------------------------------
+template <class A, class B>
+__global__ void k_real_convert(const A *__restrict__ in, B *__restrict__ out, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = (B)in[q];
+}
+// spectral: nfields padded slots (type C, pitch nfp) <-> unpadded double2
+// [nfields][n][n][nf]; TO_PADDED selects the direction
+template <class C, bool TO_PADDED>
+__global__ void k_spec_convert(C *__restrict__ padded, double2 *__restrict__ dense, Geo g,
+                               int nfields) {
+  const long long per = (long long)g.n * g.n * g.nf;
+  const long long total = per * nfields;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long f = q / per, r = q - f * per;
+    const long long row = r / g.nf;
+    const long long l = f * g.slot + row * g.nfp + (r - row * g.nf);
+    if (TO_PADDED)
+      padded[l] = from_d<C>(dense[q]);
+    else
+      dense[q] = to_d(padded[l]);
+  }
 }
 
 }  // namespace dnsb

@@ -40,7 +40,15 @@ enum {
   DNS_ERR_STATE = 6       /* call out of order (e.g. step before velocity) */
 };
 
-enum { DNS_PREC_FP64 = 0 };
+/* precision of a context:
+ *   DNS_PREC_FP64   everything in float64 (the reference's arithmetic);
+ *   DNS_PREC_MIXED  fields, FFTs and the nonlinear term in float32 (twiddles
+ *                   generated in float64/long double and rounded once); the
+ *                   energy/enstrophy reductions (double-double) and the
+ *                   pointwise update with its viscous and time-step
+ *                   coefficients computed in float64, stored in float32.
+ * Host-side arrays are float64 for both. */
+enum { DNS_PREC_FP64 = 0, DNS_PREC_MIXED = 1 };
 
 /* flags for dns_create */
 enum {
