@@ -197,6 +197,65 @@ def cpu_reference_rate(n: int, budget_s: float = 25.0):
     return rate, cores, "port", f"C restatement of main.c, {n}^3 TGV, {k} steps, {cores} threads"
 
 
+def ensemble_leg(steps: int, warmup: int):
+    """Batched ensemble: 48 runs (32 at 64^3, 16 at 128^3), nu log-uniform
+    in [1/3000, 1/100], Taylor-Green plus a seeded solenoidal perturbation
+    of rms 1e-3 of the base, FP32 fields with FP64 reductions, dt = 0.005.
+    Aggregate run-steps/s of one ensemble against the same 48 runs stepped
+    one after another as plain single-run contexts."""
+    import numpy as np
+    import torch
+
+    import dns_b200
+
+    sizes = [64] * 32 + [128] * 16
+    rng = np.random.Generator(np.random.PCG64(2024))
+    nus = np.exp(rng.uniform(np.log(1 / 3000), np.log(1 / 100), len(sizes)))
+    dt = 0.005
+    fields = {}
+    for r, n in enumerate(sizes):
+        fields[r] = dns_b200.perturbed_tgv(n, seed=r, amplitude=1e-3)
+    prec = dns_b200.DNS_PREC_MIXED
+    with dns_b200.Ensemble(sizes, prec) as ens:
+        st = torch.cuda.ExternalStream(ens.stream)
+        for r in range(len(sizes)):
+            ens.set_velocity(r, *fields[r])
+        ens.set_params(nus, dt)
+        ens.step(warmup)
+        ens.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ens.step(steps)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        d = ens.diagnostics()
+        finite = all(np.isfinite(float(a)) and np.isfinite(float(b)) for a, b in d)
+    seq_ms = {}
+    for n in (64, 128):
+        with dns_b200.Context(n, prec) as c:
+            sc = torch.cuda.ExternalStream(c.stream)
+            r = sizes.index(n)
+            c.set_velocity(*fields[r])
+            c.step(float(nus[r]), dt, warmup)
+            c.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(sc)
+            c.step(float(nus[r]), dt, steps)
+            b.record(sc)
+            b.synchronize()
+            seq_ms[n] = a.elapsed_time(b) / steps
+    agg = len(sizes) * steps / (ms / 1000.0)
+    seq = len(sizes) / ((32 * seq_ms[64] + 16 * seq_ms[128]) / 1000.0)
+    return {"runs": len(sizes), "sizes": "32x64^3 + 16x128^3", "precision": "mixed",
+            "steps": steps, "value": agg, "unit": "run-steps/s",
+            "ms_per_ensemble_step": ms / steps, "sequential_value": seq,
+            "vs_sequential": agg / seq, "all_finite": finite,
+            "seq_ms_per_step": {str(k): v for k, v in seq_ms.items()}}
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return 0
@@ -223,6 +282,7 @@ def main() -> int:
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -378,6 +438,8 @@ def main() -> int:
     h2d = 3 * n ** 3 * 8 / args.steps
     d2h = (3 * n ** 3 * 8 + 32 * ndiag) / args.steps
 
+    ens = ensemble_leg(500, args.warmup) if not args.no_ensemble else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -417,6 +479,7 @@ def main() -> int:
                     "d2h_bytes_per_step": d2h, "wall_s": wall},
             "gpu_launches": dns_b200.KERNELS_PER_STEP * args.steps,
             "mixed": mixed,
+            "ensemble": ens,
             "clocks": clk,
             "cpu_baseline": cpu,
         }

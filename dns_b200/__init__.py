@@ -75,6 +75,15 @@ _SIGS = {
     "dns_synchronize": (ctypes.c_int, [_P]),
     "dns_time_kernels": (ctypes.c_int, [_P, _D, _D, ctypes.c_long, ctypes.POINTER(_D)]),
     "dns_diagnostics_noalloc": (ctypes.c_int, [ctypes.c_long, _P, _P, _P]),
+    "dns_ens_create": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(_P)]),
+    "dns_ens_destroy": (ctypes.c_int, [_P]),
+    "dns_ens_set_velocity": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
+    "dns_ens_set_params": (ctypes.c_int, [_P, _P, _P]),
+    "dns_ens_step": (ctypes.c_int, [_P, ctypes.c_long]),
+    "dns_ens_diagnostics": (ctypes.c_int, [_P, _P]),
+    "dns_ens_get_spectral": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "dns_ens_get_stream": (_P, [_P]),
+    "dns_ens_synchronize": (ctypes.c_int, [_P]),
 }
 
 
@@ -209,6 +218,102 @@ class Context:
         ms = (ctypes.c_double * KERNELS_PER_STEP)()
         _check(self._lib.dns_time_kernels(self._h, nu, dt, nsteps, ms))
         return np.array(list(ms))
+
+
+class Ensemble:
+    """Many independent runs stepped together (mirror of dns_ens)."""
+
+    def __init__(self, sizes, precision: int = DNS_PREC_FP64, flags: int = 0):
+        self._lib = load_library()
+        self.sizes = [int(n) for n in sizes]
+        arr = (ctypes.c_long * len(self.sizes))(*self.sizes)
+        h = ctypes.c_void_p()
+        _check(self._lib.dns_ens_create(len(self.sizes), arr, precision, flags, ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dns_ens_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_velocity(self, run: int, U, V, W) -> None:
+        U, V, W = _f64(U), _f64(V), _f64(W)
+        _check(self._lib.dns_ens_set_velocity(self._h, run, _ptr(U), _ptr(V), _ptr(W)))
+
+    def set_params(self, nu, dt) -> None:
+        nu = _f64(np.broadcast_to(np.asarray(nu, dtype=np.float64), (len(self.sizes),)))
+        dt = _f64(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.sizes),)))
+        _check(self._lib.dns_ens_set_params(self._h, _ptr(nu), _ptr(dt)))
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(self._lib.dns_ens_step(self._h, nsteps))
+
+    def diagnostics(self):
+        """Per run (E, Omega) as main.c prints them."""
+        out = np.empty(4 * len(self.sizes))
+        st = self._lib.dns_ens_diagnostics(self._h, _ptr(out))
+        if st not in (DNS_OK, DNS_ERR_NONFINITE):
+            _check(st)
+        return [scale_diagnostics(*out[4 * r:4 * r + 4], n) for r, n in enumerate(self.sizes)]
+
+    def get_spectral(self, run: int) -> np.ndarray:
+        n = self.sizes[run]
+        out = np.empty((3, n, n, n // 2 + 1), dtype=np.complex128)
+        _check(self._lib.dns_ens_get_spectral(self._h, run, _ptr(out)))
+        return out
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.dns_ens_get_stream(self._h) or 0)
+
+    def synchronize(self) -> None:
+        _check(self._lib.dns_ens_synchronize(self._h))
+
+
+def solenoidal_perturbation(n: int, seed: int, k0: float = 4.0):
+    """Seeded random divergence-free velocity with energy spectrum
+    E(k) ~ k^4 exp(-2 (k/k0)^2): white Gaussian noise (numpy PCG64(seed)),
+    forward transform, amplitude sqrt(E(k)) / k per mode, projection onto
+    k-perpendicular, back transform.  Returned with unit rms."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k1 = np.fft.fftfreq(n, 1.0 / n)
+    kz = np.arange(n // 2 + 1, dtype=np.float64)
+    KX, KY, KZ = np.meshgrid(k1, k1, kz, indexing="ij")
+    kk = KX ** 2 + KY ** 2 + KZ ** 2
+    kmag = np.sqrt(kk)
+    amp = np.where(kmag > 0, kmag * np.exp(-((kmag / k0) ** 2)), 0.0)  # sqrt(E)/k
+    # no Nyquist content (its derivative is ambiguous on the half spectrum)
+    nyq = (np.abs(KX) == n // 2) | (np.abs(KY) == n // 2) | (KZ == n // 2)
+    amp[nyq] = 0.0
+    hats = [np.fft.rfftn(rng.standard_normal((n, n, n))) * amp for _ in range(3)]
+    div = (KX * hats[0] + KY * hats[1] + KZ * hats[2]) / np.where(kk > 0, kk, 1.0)
+    hats = [hats[0] - KX * div, hats[1] - KY * div, hats[2] - KZ * div]
+    u = [np.fft.irfftn(h, s=(n, n, n), axes=(0, 1, 2)) for h in hats]
+    rms = np.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2))
+    return [c / rms for c in u]
+
+
+def perturbed_tgv(n: int, seed: int, amplitude: float = 1e-3):
+    """Taylor-Green plus a seeded solenoidal perturbation whose rms is
+    `amplitude` times the rms of the Taylor-Green field (the ensemble
+    configuration's initial fields)."""
+    U, V, W, _ = tgv_fields(n)
+    rms_tgv = np.sqrt(np.mean(U ** 2 + V ** 2 + W ** 2))
+    d = solenoidal_perturbation(n, seed)
+    s = amplitude * rms_tgv
+    return U + s * d[0], V + s * d[1], W + s * d[2]
 
 
 def scale_diagnostics(eh, el, oh, ol, n):

@@ -85,33 +85,69 @@ namespace dnsb {
 void set_last_error(const char *msg) { g_last_error = msg; }
 }  // namespace dnsb
 
-struct dns_ctx {
+// A group: nruns runs of one grid size and precision in one arena, stepped
+// by the same (batched) kernel launches.  A dns_ctx is a group of one run;
+// a dns_ens holds one group per distinct grid size.
+struct Group {
   long n = 0;
   int precision = 0;
   unsigned flags = 0;
-  int device = 0;
+  int nruns = 1;
   size_t csize = 16;      // bytes of one complex element
   size_t rsize = 8;       // bytes of one real element
   Geo g{};
-  cudaStream_t stream = nullptr;
   char *arena = nullptr;
   size_t arena_bytes = 0;
-  void *S = nullptr;      // spectral slots
-  void *stale = nullptr;  // stale real velocity
+  void *S = nullptr;      // spectral slots [nruns][NSLOTS][slot]
+  void *stale = nullptr;  // stale real velocity [nruns][3][n^3]
   void *tw = nullptr;     // twiddles exp(-2 pi i k / n)
-  double4 *diag_part = nullptr, *diag_out = nullptr;
+  double4 *diag_part = nullptr;  // [nruns][diag_blocks]
+  double4 *diag_out = nullptr;   // [nruns]
+  double *coef = nullptr;        // [nruns][2]: nu, dt
   int diag_blocks = 0;
+  double *realbuf = nullptr;     // [4][n^3] float64, allocated on first field read
+
+  char *slot_ptr(int run, int s) const {
+    return (char *)S + ((size_t)run * g.run_spec + (size_t)s * g.slot) * csize;
+  }
+  // float64 staging for host transfers of the FP32 path: the run's work
+  // slots (7 * n^2 * nfp * 8 bytes >= 3 n^3 * 8 and >= 3 n^2 nf * 16)
+  double *staging(int run) const { return (double *)slot_ptr(run, SLOT_WORK); }
+  // the same arena seen as a batch of one run
+  Group one(int run) const {
+    Group v = *this;
+    v.nruns = 1;
+    v.S = slot_ptr(run, 0);
+    v.stale = (char *)stale + (size_t)run * g.run_real * rsize;
+    v.diag_part = diag_part + (size_t)run * diag_blocks;
+    v.diag_out = diag_out + run;
+    v.coef = coef + 2 * run;
+    return v;
+  }
+};
+
+struct dns_ctx {
+  Group grp;
+  cudaStream_t stream = nullptr;
   double4 *diag_host = nullptr;  // pinned
-  double *realbuf = nullptr;     // [4][n^3] float64, allocated on first dns_get_fields
   bool have_state = false;
   cudaGraphExec_t graph = nullptr;
-  double graph_nu = 0, graph_dt = 0;
+  double cur_nu = NAN, cur_dt = NAN;
   int kernels_per_step = 4 * KERNELS_PER_STAGE;
+};
 
-  char *slot_ptr(int s) const { return (char *)S + (size_t)s * g.slot * csize; }
-  // float64 staging for host transfers of the FP32 path: the work slots
-  // (7 * n^2 * nfp * 8 bytes >= 3 n^3 * 8 and >= 3 n^2 nf * 16)
-  double *staging() const { return (double *)slot_ptr(SLOT_WORK); }
+struct dns_ens {
+  std::vector<Group> groups;
+  std::vector<int> run_group, run_index;  // run -> (group, index in group)
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> gstreams;
+  std::vector<cudaEvent_t> gevents;
+  cudaEvent_t fork = nullptr;
+  double4 *diag_host = nullptr;  // pinned [nruns]
+  std::vector<char> have_state;
+  cudaGraphExec_t graph = nullptr;
+  int nruns = 0;
+  bool params_set = false;
 };
 
 namespace {
@@ -119,13 +155,14 @@ namespace {
 constexpr double RK_A[4] = {1 / 6.0, 1 / 3.0, 1 / 3.0, 1 / 6.0};  // main.c:15
 constexpr double RK_B[3] = {0.5, 0.5, 1.0};                       // main.c:16
 
-ColJobs jobs_empty() {
+ColJobs jobs_empty(int njobs) {
   ColJobs j;
   for (int q = 0; q < 8; q++) j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1;
+  j.njobs = njobs;
   return j;
 }
 ColJobs jobs_pass_a(int in0) {
-  ColJobs j = jobs_empty();
+  ColJobs j = jobs_empty(3);
   const int w = SLOT_WORK;
   j.in_slot[0] = in0 + 0; j.out_slot[0] = w + SU;
   j.in_slot[1] = in0 + 1; j.out_slot[1] = w + SV; j.der_slot[1] = w + SDVDX;
@@ -133,7 +170,7 @@ ColJobs jobs_pass_a(int in0) {
   return j;
 }
 ColJobs jobs_pass_b(bool first) {
-  ColJobs j = jobs_empty();
+  ColJobs j = jobs_empty(5);
   const int w = SLOT_WORK;
   j.in_slot[0] = w + SU; j.out_slot[0] = w + SU; j.der_slot[0] = w + SDUDY;
   j.in_slot[1] = w + SV; j.out_slot[1] = w + SV;
@@ -144,7 +181,7 @@ ColJobs jobs_pass_b(bool first) {
   return j;
 }
 ColJobs jobs_map(const int *in, const int *out, int cnt) {
-  ColJobs j = jobs_empty();
+  ColJobs j = jobs_empty(cnt);
   for (int q = 0; q < cnt; q++) j.in_slot[q] = in[q], j.out_slot[q] = out[q];
   return j;
 }
@@ -177,102 +214,103 @@ struct Ops {
     return cudaSuccess;
   }
 
-  static C *S(dns_ctx *c) { return (C *)c->S; }
-  static C *slot(dns_ctx *c, int s) { return S(c) + (long long)s * c->g.slot; }
-  static const C *tw(dns_ctx *c) { return (const C *)c->tw; }
+  static C *slot(const Group &G, int s) { return (C *)G.S + (long long)s * G.g.slot; }
+  static const C *tw(const Group &G) { return (const C *)G.tw; }
 
   template <int AXIS, bool FWD>
-  static void colpass(dns_ctx *c, const ColJobs &jobs, int njobs) {
-    dim3 grid(c->g.nfp / W, N, njobs);
-    k_colpass<R, N, AXIS, FWD><<<grid, CT, COL_SMEM, c->stream>>>(S(c), S(c), tw(c), c->g, jobs);
+  static void colpass(const Group &G, cudaStream_t st, const ColJobs &jobs) {
+    dim3 grid(G.g.nfp / W, N, jobs.njobs * G.nruns);
+    k_colpass<R, N, AXIS, FWD><<<grid, CT, COL_SMEM, st>>>((C *)G.S, (C *)G.S, tw(G), G.g, jobs);
   }
 
   static dim3 zgrid(int nfields) { return dim3((N * N) / ZCfg<N>::LINES, nfields); }
-  static dim3 zsgrid() { return dim3((N * N + ZC<R, N>::LINES - 1) / ZC<R, N>::LINES); }
+  static dim3 zsgrid(int nruns) {
+    return dim3((N * N + ZC<R, N>::LINES - 1) / ZC<R, N>::LINES, nruns);
+  }
 
-  // kernel `k` (0..KERNELS_PER_STAGE-1) of RK stage `s`
-  static void stage_kernel(dns_ctx *c, int s, int k, double nu, double dt) {
-    const Geo &g = c->g;
-    C *work = slot(c, SLOT_WORK);
-    R *stale = (R *)c->stale;
+  // kernel `k` (0..KERNELS_PER_STAGE-1) of RK stage `s`, all runs of G
+  static void stage_kernel(const Group &G, cudaStream_t st, int s, int k) {
+    const Geo &g = G.g;
+    C *work = slot(G, SLOT_WORK);
+    R *stale = (R *)G.stale;
     const R invn3 = (R)(1.0 / (double)g.nreal);
     switch (k) {
       case 0:
-        colpass<0, false>(c, jobs_pass_a(s == 0 ? SLOT_SA : SLOT_SB), 3);
+        colpass<0, false>(G, st, jobs_pass_a(s == 0 ? SLOT_SA : SLOT_SB));
         break;
       case 1:
-        colpass<1, false>(c, jobs_pass_b(s == 0), 5);
+        colpass<1, false>(G, st, jobs_pass_b(s == 0));
         break;
       case 2:
         if (s == 0)
-          k_zstage<R, N, 0><<<zsgrid(), ZC<R, N>::THREADS, ZS_SMEM, c->stream>>>(work, stale, tw(c), g, invn3);
+          k_zstage<R, N, 0><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
         else if (s < 3)
-          k_zstage<R, N, 1><<<zsgrid(), ZC<R, N>::THREADS, ZS_SMEM, c->stream>>>(work, stale, tw(c), g, invn3);
+          k_zstage<R, N, 1><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
         else
-          k_zstage<R, N, 2><<<zsgrid(), ZC<R, N>::THREADS, ZS_SMEM, c->stream>>>(work, stale, tw(c), g, invn3);
+          k_zstage<R, N, 2><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
         break;
       case 3:
       case 4: {
         // D: y forward, E1: x forward (in place on the three N slots)
         const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
         if (k == 3)
-          colpass<1, true>(c, jobs_map(io, io, 3), 3);
+          colpass<1, true>(G, st, jobs_map(io, io, 3));
         else
-          colpass<0, true>(c, jobs_map(io, io, 3), 3);
+          colpass<0, true>(G, st, jobs_map(io, io, 3));
         break;
       }
       default: {
         StageArgs<R> sa;
-        sa.u0 = slot(c, SLOT_SA);
-        sa.us = slot(c, s == 0 ? SLOT_SA : SLOT_SB);
-        sa.acc = slot(c, SLOT_ACC);
-        sa.next = slot(c, SLOT_SB);
-        sa.ph = (s == 3 && (c->flags & DNS_FLAG_PRESSURE)) ? slot(c, SLOT_P) : nullptr;
-        sa.nu = nu;
-        sa.dt = dt;
+        sa.u0 = slot(G, SLOT_SA);
+        sa.us = slot(G, s == 0 ? SLOT_SA : SLOT_SB);
+        sa.acc = slot(G, SLOT_ACC);
+        sa.next = slot(G, SLOT_SB);
+        sa.ph = (s == 3 && (G.flags & DNS_FLAG_PRESSURE)) ? slot(G, SLOT_P) : nullptr;
+        sa.coef = G.coef;
         sa.a = RK_A[s];
         sa.b = s < 3 ? RK_B[s] : 0.0;
         const long long npts = (long long)N * N * g.nf;
-        const int per = UPD_THREADS * UPD_PER_THREAD;
-        dim3 grid((unsigned)((npts + per - 1) / per));
+        const int per = UPD_THREADS * UpdPer<R>::V;
+        dim3 grid((unsigned)((npts + per - 1) / per), G.nruns);
         switch (s) {
-          case 0: k_update<R, 0><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
-          case 1: k_update<R, 1><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
-          case 2: k_update<R, 2><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
-          default: k_update<R, 3><<<grid, UPD_THREADS, 0, c->stream>>>(work, g, sa); break;
+          case 0: k_update<R, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          case 1: k_update<R, 1><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          case 2: k_update<R, 2><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          default: k_update<R, 3><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
         }
       }
     }
   }
 
-  static void step(dns_ctx *c, double nu, double dt) {
+  static void step(const Group &G, cudaStream_t st) {
     for (int s = 0; s < 4; s++)
-      for (int k = 0; k < KERNELS_PER_STAGE; k++) stage_kernel(c, s, k, nu, dt);
+      for (int k = 0; k < KERNELS_PER_STAGE; k++) stage_kernel(G, st, s, k);
   }
 
-  // forward transform of the three stale real slots into SA
-  static void forward(dns_ctx *c) {
-    k_zr2c<R, N><<<zgrid(3), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>((const R *)c->stale,
-                                                                     slot(c, SLOT_WORK), tw(c), c->g);
+  // forward transform of the three stale real slots into SA (one run)
+  static void forward(const Group &G, cudaStream_t st) {
+    k_zr2c<R, N><<<zgrid(3), ZCfg<N>::THREADS, Z_SMEM, st>>>((const R *)G.stale,
+                                                              slot(G, SLOT_WORK), tw(G), G.g);
     const int w3[3] = {SLOT_WORK + 0, SLOT_WORK + 1, SLOT_WORK + 2};
     const int sa[3] = {SLOT_SA + 0, SLOT_SA + 1, SLOT_SA + 2};
-    colpass<1, true>(c, jobs_map(w3, w3, 3), 3);
-    colpass<0, true>(c, jobs_map(w3, sa, 3), 3);
+    colpass<1, true>(G, st, jobs_map(w3, w3, 3));
+    colpass<0, true>(G, st, jobs_map(w3, sa, 3));
   }
 
-  // c2r(X) / n^3 of SA (and P) into realbuf [4][n^3] float64
-  static void backward(dns_ctx *c, int nfields) {
+  // c2r(X) / n^3 of SA (and P) into realbuf [4][n^3] float64 (one run)
+  static void backward(const Group &G, cudaStream_t st, int nfields) {
     const int in[4] = {SLOT_SA + 0, SLOT_SA + 1, SLOT_SA + 2, SLOT_P};
     const int w4[4] = {SLOT_WORK + 0, SLOT_WORK + 1, SLOT_WORK + 2, SLOT_WORK + 3};
-    colpass<0, false>(c, jobs_map(in, w4, nfields), nfields);
-    colpass<1, false>(c, jobs_map(w4, w4, nfields), nfields);
-    k_zc2r<R, N><<<zgrid(nfields), ZCfg<N>::THREADS, Z_SMEM, c->stream>>>(
-        slot(c, SLOT_WORK), c->realbuf, tw(c), c->g, 1.0 / (double)c->g.nreal);
+    colpass<0, false>(G, st, jobs_map(in, w4, nfields));
+    colpass<1, false>(G, st, jobs_map(w4, w4, nfields));
+    k_zc2r<R, N><<<zgrid(nfields), ZCfg<N>::THREADS, Z_SMEM, st>>>(
+        slot(G, SLOT_WORK), G.realbuf, tw(G), G.g, 1.0 / (double)G.g.nreal);
   }
 
-  static void diag(dns_ctx *c) {
-    k_diag<256, C><<<c->diag_blocks, 256, 0, c->stream>>>(slot(c, SLOT_SA), c->g, c->diag_part);
-    k_diag_final<256><<<1, 256, 0, c->stream>>>(c->diag_part, c->diag_blocks, c->diag_out);
+  // energy / enstrophy sums of every run into diag_out[run]
+  static void diag(const Group &G, cudaStream_t st) {
+    k_diag<256, C><<<dim3(G.diag_blocks, G.nruns), 256, 0, st>>>(slot(G, SLOT_SA), G.g, G.diag_part);
+    k_diag_final<256><<<G.nruns, 256, 0, st>>>(G.diag_part, G.diag_blocks, G.diag_out);
   }
 };
 
@@ -296,8 +334,8 @@ bool dispatch_n(int prec, long n, F &&f) {
   return false;
 }
 template <class F>
-bool dispatch(dns_ctx *c, F &&f) {
-  return dispatch_n(c->precision, c->n, f);
+bool dispatch(const Group &G, F &&f) {
+  return dispatch_n(G.precision, G.n, f);
 }
 
 int check_launch(const char *file, int line) {
@@ -311,15 +349,173 @@ int check_launch(const char *file, int line) {
     if (st_ != DNS_OK) return st_;                     \
   } while (0)
 
-int build_graph(dns_ctx *c, double nu, double dt) {
-  if (c->graph && c->graph_nu == nu && c->graph_dt == dt) return DNS_OK;
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
+unsigned conv_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  return (unsigned)(b < 148 * 16 ? b : 148 * 16);
+}
+
+void group_free(Group &G) {
+  if (G.realbuf) cudaFree(G.realbuf);
+  if (G.arena) cudaFree(G.arena);
+  G.realbuf = nullptr;
+  G.arena = nullptr;
+}
+
+// allocate and initialise the arena of a group (synchronous on `st`)
+int group_init(Group &G, long n, int precision, unsigned flags, int nruns, cudaStream_t st) {
+  if (precision != DNS_PREC_FP64 && precision != DNS_PREC_MIXED)
+    return fail(DNS_ERR_UNSUPPORTED, "precision not supported", __FILE__, __LINE__);
+  if (nruns < 1) return fail(DNS_ERR_ARG, "nruns < 1", __FILE__, __LINE__);
+  cudaError_t se = cudaErrorInvalidValue;
+  if (!dispatch_n(precision, n, [&](auto ops) { se = decltype(ops)::setup(); })) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "n = %ld is not supported (powers of two 8..512)", n);
+    return fail(DNS_ERR_UNSUPPORTED, buf, __FILE__, __LINE__);
   }
+  CK(se);
+  G.n = n;
+  G.precision = precision;
+  G.flags = flags;
+  G.nruns = nruns;
+  const bool fp64 = precision == DNS_PREC_FP64;
+  G.csize = fp64 ? sizeof(double2) : sizeof(float2);
+  G.rsize = fp64 ? sizeof(double) : sizeof(float);
+  const int W = fp64 ? ColW<double>::W : ColW<float>::W;
+  Geo &g = G.g;
+  g.n = (int)n;
+  g.nf = (int)(n / 2 + 1);
+  g.nfp = (g.nf + W - 1) / W * W;
+  g.slot = (long long)n * n * g.nfp;
+  g.nreal = (long long)n * n * n;
+  g.run_spec = g.slot * NSLOTS;
+  g.run_real = 3 * g.nreal;
+  // 2/3 rule of main.c:231-238: keep |k| < kmax with kmax = 2/3 (n/2 + 1)
+  const double kmax = 2. / 3. * (n / 2 + 1);
+  int kcut = -1;
+  while ((double)(kcut + 1) < kmax) kcut++;
+  g.kcut = kcut;
+  const long long npts = (long long)n * n * g.nf;
+  G.diag_blocks = (int)((npts + 255) / 256 < 1184 ? (npts + 255) / 256 : 1184);
+
+  const size_t spec_b = (size_t)g.run_spec * G.csize * nruns;
+  const size_t stale_b = (size_t)g.run_real * G.rsize * nruns;
+  const size_t tw_b = (size_t)n * G.csize;
+  const size_t part_b = (size_t)(G.diag_blocks + 1) * nruns * sizeof(double4);
+  const size_t coef_b = (size_t)2 * nruns * sizeof(double);
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  G.arena_bytes = al(spec_b) + al(stale_b) + al(tw_b) + al(part_b) + al(coef_b);
+  cudaError_t e = cudaMalloc((void **)&G.arena, G.arena_bytes);
+  if (e != cudaSuccess) {
+    G.arena = nullptr;
+    return fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  char *p = G.arena;
+  G.S = p; p += al(spec_b);
+  G.stale = p; p += al(stale_b);
+  G.tw = p; p += al(tw_b);
+  G.diag_part = (double4 *)p; p += al(part_b);
+  G.diag_out = G.diag_part + (size_t)G.diag_blocks * nruns;
+  G.coef = (double *)p;
+  // twiddles exp(-2 pi i k / n), generated in long double, rounded once to
+  // the storage precision
+  std::vector<double2> twd(n);
+  std::vector<float2> twf(n);
+  for (long k = 0; k < n; k++) {
+    double cs, sn;
+    sincos2pi(k, n, &cs, &sn);
+    twd[k] = make_double2(cs, -sn);
+    twf[k] = make_float2((float)cs, (float)-sn);
+  }
+  std::vector<double> coef(2 * nruns, 0.0);
+  const void *src = fp64 ? (const void *)twd.data() : (const void *)twf.data();
+  CK(cudaMemcpyAsync(G.tw, src, tw_b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(G.coef, coef.data(), coef_b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(G.S, 0, spec_b, st));
+  CK(cudaMemsetAsync(G.stale, 0, stale_b, st));
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
+// host float64 [3][n^3] -> stale real slots of a one-run view
+int upload_real3(const Group &G, cudaStream_t st, const double *const src[3]) {
+  const long long nr = G.g.nreal;
+  const size_t fb = (size_t)nr * sizeof(double);
+  double *dst = G.precision == DNS_PREC_FP64 ? (double *)G.stale : G.staging(0);
+  for (int f = 0; f < 3; f++)
+    CK(cudaMemcpyAsync(dst + f * nr, src[f], fb, cudaMemcpyHostToDevice, st));
+  if (G.precision != DNS_PREC_FP64) {
+    k_real_convert<double, float><<<conv_blocks(3 * nr), 256, 0, st>>>(dst, (float *)G.stale, 3 * nr);
+    CKL();
+  }
+  return DNS_OK;
+}
+
+// velocity of one run: upload and transform
+int set_velocity_view(const Group &V, cudaStream_t st, const double *U, const double *Vv,
+                      const double *W) {
+  const double *src[3] = {U, Vv, W};
+  int s = upload_real3(V, st, src);
+  if (s != DNS_OK) return s;
+  dispatch(V, [&](auto ops) { decltype(ops)::forward(V, st); });
+  CKL();
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
+int get_spectral_view(const Group &V, cudaStream_t st, double *uvw) {
+  const Geo &g = V.g;
+  const size_t row = (size_t)g.nf * sizeof(double2);
+  const size_t rows = (size_t)g.n * g.n;
+  if (V.precision == DNS_PREC_FP64) {
+    const size_t pitch = (size_t)g.nfp * sizeof(double2);
+    for (int f = 0; f < 3; f++)
+      CK(cudaMemcpy2DAsync((char *)uvw + f * rows * row, row, V.slot_ptr(0, SLOT_SA + f), pitch, row,
+                           rows, cudaMemcpyDeviceToHost, st));
+  } else {
+    const long long tot = 3LL * g.n * g.n * g.nf;
+    k_spec_convert<float2, false><<<conv_blocks(tot), 256, 0, st>>>(
+        (float2 *)V.slot_ptr(0, SLOT_SA), (double2 *)V.staging(0), g, 3);
+    CKL();
+    CK(cudaMemcpyAsync(uvw, V.staging(0), 3 * rows * row, cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
+int set_spectral_view(const Group &V, cudaStream_t st, const double *uvw) {
+  const Geo &g = V.g;
+  const size_t row = (size_t)g.nf * sizeof(double2);
+  const size_t rows = (size_t)g.n * g.n;
+  if (V.precision == DNS_PREC_FP64) {
+    const size_t pitch = (size_t)g.nfp * sizeof(double2);
+    for (int f = 0; f < 3; f++)
+      CK(cudaMemcpy2DAsync(V.slot_ptr(0, SLOT_SA + f), pitch, (const char *)uvw + f * rows * row, row,
+                           row, rows, cudaMemcpyHostToDevice, st));
+  } else {
+    const long long tot = 3LL * g.n * g.n * g.nf;
+    CK(cudaMemcpyAsync(V.staging(0), uvw, 3 * rows * row, cudaMemcpyHostToDevice, st));
+    k_spec_convert<float2, true><<<conv_blocks(tot), 256, 0, st>>>(
+        (float2 *)V.slot_ptr(0, SLOT_SA), (double2 *)V.staging(0), g, 3);
+    CKL();
+  }
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
+// coefficients nu, dt of every run of a group (host arrays of nruns)
+int set_coef(const Group &G, cudaStream_t st, const double *nu, const double *dt) {
+  std::vector<double> c(2 * G.nruns);
+  for (int r = 0; r < G.nruns; r++) c[2 * r] = nu[r], c[2 * r + 1] = dt[r];
+  CK(cudaMemcpyAsync(G.coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
+int ctx_build_graph(dns_ctx *c) {
+  if (c->graph) return DNS_OK;
   cudaGraph_t gr;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  dispatch(c, [&](auto ops) { decltype(ops)::step(c, nu, dt); });
+  dispatch(c->grp, [&](auto ops) { decltype(ops)::step(c->grp, c->stream); });
   cudaError_t le = cudaGetLastError();
   cudaError_t ce = cudaStreamEndCapture(c->stream, &gr);
   if (le != cudaSuccess) return fail(DNS_ERR_CUDA, cudaGetErrorString(le), __FILE__, __LINE__);
@@ -327,27 +523,6 @@ int build_graph(dns_ctx *c, double nu, double dt) {
   cudaError_t ie = cudaGraphInstantiate(&c->graph, gr, 0);
   cudaGraphDestroy(gr);
   CK(ie);
-  c->graph_nu = nu;
-  c->graph_dt = dt;
-  return DNS_OK;
-}
-
-unsigned conv_blocks(long long n) {
-  long long b = (n + 255) / 256;
-  return (unsigned)(b < 148 * 16 ? b : 148 * 16);
-}
-
-// host float64 [3][n^3] -> stale real slots (converted for the FP32 path)
-int upload_real3(dns_ctx *c, const double *const src[3]) {
-  const long long nr = c->g.nreal;
-  const size_t fb = (size_t)nr * sizeof(double);
-  double *dst = c->precision == DNS_PREC_FP64 ? (double *)c->stale : c->staging();
-  for (int f = 0; f < 3; f++)
-    CK(cudaMemcpyAsync(dst + f * nr, src[f], fb, cudaMemcpyHostToDevice, c->stream));
-  if (c->precision != DNS_PREC_FP64) {
-    k_real_convert<double, float><<<conv_blocks(3 * nr), 256, 0, c->stream>>>(dst, (float *)c->stale, 3 * nr);
-    CKL();
-  }
   return DNS_OK;
 }
 
@@ -373,79 +548,19 @@ const char *dns_last_error(void) { return g_last_error.c_str(); }
 int dns_create(long n, int precision, unsigned flags, dns_ctx **out) {
   if (!out) return fail(DNS_ERR_ARG, "out is NULL", __FILE__, __LINE__);
   *out = nullptr;
-  if (precision != DNS_PREC_FP64 && precision != DNS_PREC_MIXED)
-    return fail(DNS_ERR_UNSUPPORTED, "precision not supported", __FILE__, __LINE__);
-  cudaError_t se = cudaErrorInvalidValue;
-  if (!dispatch_n(precision, n, [&](auto ops) { se = decltype(ops)::setup(); })) {
-    char buf[128];
-    snprintf(buf, sizeof buf, "n = %ld is not supported (powers of two 8..512)", n);
-    return fail(DNS_ERR_UNSUPPORTED, buf, __FILE__, __LINE__);
-  }
-  CK(se);
   dns_ctx *c = new dns_ctx();
-  c->n = n;
-  c->precision = precision;
-  c->flags = flags;
-  const bool fp64 = precision == DNS_PREC_FP64;
-  c->csize = fp64 ? sizeof(double2) : sizeof(float2);
-  c->rsize = fp64 ? sizeof(double) : sizeof(float);
-  const int W = fp64 ? ColW<double>::W : ColW<float>::W;
-  cudaGetDevice(&c->device);
-  Geo &g = c->g;
-  g.n = (int)n;
-  g.nf = (int)(n / 2 + 1);
-  g.nfp = (g.nf + W - 1) / W * W;
-  g.slot = (long long)n * n * g.nfp;
-  g.nreal = (long long)n * n * n;
-  // 2/3 rule of main.c:231-238: keep |k| < kmax with kmax = 2/3 (n/2 + 1)
-  const double kmax = 2. / 3. * (n / 2 + 1);
-  int kcut = -1;
-  while ((double)(kcut + 1) < kmax) kcut++;
-  g.kcut = kcut;
-  const long long npts = (long long)n * n * g.nf;
-  c->diag_blocks = (int)((npts + 255) / 256 < 1184 ? (npts + 255) / 256 : 1184);
-
-  const size_t slot_b = (size_t)g.slot * c->csize;
-  const size_t spec_b = slot_b * NSLOTS;
-  const size_t stale_b = (size_t)g.nreal * 3 * c->rsize;
-  const size_t tw_b = (size_t)n * c->csize;
-  const size_t part_b = (size_t)c->diag_blocks * sizeof(double4) + sizeof(double4);
-  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-  c->arena_bytes = al(spec_b) + al(stale_b) + al(tw_b) + al(part_b);
-  cudaError_t e = cudaMalloc((void **)&c->arena, c->arena_bytes);
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
-    return fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
+    return fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
-  char *p = c->arena;
-  c->S = p; p += al(spec_b);
-  c->stale = p; p += al(stale_b);
-  c->tw = p; p += al(tw_b);
-  c->diag_part = (double4 *)p;
-  c->diag_out = c->diag_part + c->diag_blocks;
-  int st = DNS_OK;
-  do {
-    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking))) break;
-    if ((e = cudaMallocHost((void **)&c->diag_host, sizeof(double4)))) break;
-    // twiddles exp(-2 pi i k / n), generated in long double, rounded once to
-    // the storage precision
-    std::vector<double2> twd(n);
-    std::vector<float2> twf(n);
-    for (long k = 0; k < n; k++) {
-      double cs, sn;
-      sincos2pi(k, n, &cs, &sn);
-      twd[k] = make_double2(cs, -sn);
-      twf[k] = make_float2((float)cs, (float)-sn);
-    }
-    const void *src = fp64 ? (const void *)twd.data() : (const void *)twf.data();
-    if ((e = cudaMemcpyAsync(c->tw, src, tw_b, cudaMemcpyHostToDevice, c->stream))) break;
-    if ((e = cudaMemsetAsync(c->S, 0, spec_b, c->stream))) break;
-    if ((e = cudaMemsetAsync(c->stale, 0, stale_b, c->stream))) break;
-    if ((e = cudaStreamSynchronize(c->stream))) break;
-  } while (0);
-  if (e != cudaSuccess) {
-    st = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  int st = group_init(c->grp, n, precision, flags, 1, c->stream);
+  if (st == DNS_OK && cudaMallocHost((void **)&c->diag_host, sizeof(double4)) != cudaSuccess)
+    st = fail(DNS_ERR_NOMEM, "pinned host allocation failed", __FILE__, __LINE__);
+  if (st != DNS_OK) {
+    std::string keep = g_last_error;
     dns_destroy(c);
+    g_last_error = keep;
     return st;
   }
   *out = c;
@@ -456,9 +571,8 @@ int dns_destroy(dns_ctx *c) {
   if (!c) return DNS_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
-  if (c->realbuf) cudaFree(c->realbuf);
+  group_free(c->grp);
   if (c->diag_host) cudaFreeHost(c->diag_host);
-  if (c->arena) cudaFree(c->arena);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DNS_OK;
@@ -466,21 +580,22 @@ int dns_destroy(dns_ctx *c) {
 
 int dns_set_velocity(dns_ctx *c, const double *U, const double *V, const double *W) {
   if (!c || !U || !V || !W) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  const double *src[3] = {U, V, W};
-  int st = upload_real3(c, src);
-  if (st != DNS_OK) return st;
-  dispatch(c, [&](auto ops) { decltype(ops)::forward(c); });
-  CKL();
-  CK(cudaStreamSynchronize(c->stream));
-  c->have_state = true;
-  return DNS_OK;
+  int st = set_velocity_view(c->grp, c->stream, U, V, W);
+  if (st == DNS_OK) c->have_state = true;
+  return st;
 }
 
 int dns_step(dns_ctx *c, double nu, double dt, long nsteps) {
   if (!c || nsteps < 0) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
   if (!c->have_state) return fail(DNS_ERR_STATE, "no velocity set", __FILE__, __LINE__);
   if (nsteps == 0) return DNS_OK;
-  int st = build_graph(c, nu, dt);
+  if (!(nu == c->cur_nu && dt == c->cur_dt)) {
+    int st = set_coef(c->grp, c->stream, &nu, &dt);
+    if (st != DNS_OK) return st;
+    c->cur_nu = nu;
+    c->cur_dt = dt;
+  }
+  int st = ctx_build_graph(c);
   if (st != DNS_OK) return st;
   for (long s = 0; s < nsteps; s++) CK(cudaGraphLaunch(c->graph, c->stream));
   return DNS_OK;
@@ -488,9 +603,10 @@ int dns_step(dns_ctx *c, double nu, double dt, long nsteps) {
 
 int dns_diagnostics(dns_ctx *c, double *e_hi, double *e_lo, double *om_hi, double *om_lo) {
   if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
-  dispatch(c, [&](auto ops) { decltype(ops)::diag(c); });
+  dispatch(c->grp, [&](auto ops) { decltype(ops)::diag(c->grp, c->stream); });
   CKL();
-  CK(cudaMemcpyAsync(c->diag_host, c->diag_out, sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->diag_host, c->grp.diag_out, sizeof(double4), cudaMemcpyDeviceToHost,
+                     c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const double4 r = *c->diag_host;
   if (e_hi) *e_hi = r.x;
@@ -504,73 +620,45 @@ int dns_diagnostics(dns_ctx *c, double *e_hi, double *e_lo, double *om_hi, doubl
 
 int dns_get_fields(dns_ctx *c, double *U, double *V, double *W, double *P) {
   if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
-  if (P && !(c->flags & DNS_FLAG_PRESSURE))
+  Group &G = c->grp;
+  if (P && !(G.flags & DNS_FLAG_PRESSURE))
     return fail(DNS_ERR_ARG, "P requested without DNS_FLAG_PRESSURE", __FILE__, __LINE__);
-  const size_t fb = (size_t)c->g.nreal * sizeof(double);
-  if (!c->realbuf) CK(cudaMalloc((void **)&c->realbuf, 4 * fb));
+  const size_t fb = (size_t)G.g.nreal * sizeof(double);
+  if (!G.realbuf) CK(cudaMalloc((void **)&G.realbuf, 4 * fb));
   const int nf = P ? 4 : 3;
-  dispatch(c, [&](auto ops) { decltype(ops)::backward(c, nf); });
+  dispatch(G, [&](auto ops) { decltype(ops)::backward(G, c->stream, nf); });
   CKL();
   double *dst[4] = {U, V, W, P};
   for (int f = 0; f < nf; f++)
     if (dst[f])
-      CK(cudaMemcpyAsync(dst[f], c->realbuf + f * c->g.nreal, fb, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(dst[f], G.realbuf + f * G.g.nreal, fb, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DNS_OK;
 }
 
 int dns_get_spectral(dns_ctx *c, double *uvw) {
   if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  const Geo &g = c->g;
-  const size_t row = (size_t)g.nf * sizeof(double2);
-  const size_t rows = (size_t)g.n * g.n;
-  if (c->precision == DNS_PREC_FP64) {
-    const size_t pitch = (size_t)g.nfp * sizeof(double2);
-    for (int f = 0; f < 3; f++)
-      CK(cudaMemcpy2DAsync((char *)uvw + f * rows * row, row, c->slot_ptr(SLOT_SA + f), pitch, row,
-                           rows, cudaMemcpyDeviceToHost, c->stream));
-  } else {
-    const long long tot = 3LL * g.n * g.n * g.nf;
-    k_spec_convert<float2, false><<<conv_blocks(tot), 256, 0, c->stream>>>(
-        (float2 *)c->slot_ptr(SLOT_SA), (double2 *)c->staging(), g, 3);
-    CKL();
-    CK(cudaMemcpyAsync(uvw, c->staging(), 3 * rows * row, cudaMemcpyDeviceToHost, c->stream));
-  }
-  CK(cudaStreamSynchronize(c->stream));
-  return DNS_OK;
+  return get_spectral_view(c->grp, c->stream, uvw);
 }
 
 int dns_set_spectral(dns_ctx *c, const double *uvw) {
   if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  const Geo &g = c->g;
-  const size_t row = (size_t)g.nf * sizeof(double2);
-  const size_t rows = (size_t)g.n * g.n;
-  if (c->precision == DNS_PREC_FP64) {
-    const size_t pitch = (size_t)g.nfp * sizeof(double2);
-    for (int f = 0; f < 3; f++)
-      CK(cudaMemcpy2DAsync(c->slot_ptr(SLOT_SA + f), pitch, (const char *)uvw + f * rows * row, row,
-                           row, rows, cudaMemcpyHostToDevice, c->stream));
-  } else {
-    const long long tot = 3LL * g.n * g.n * g.nf;
-    CK(cudaMemcpyAsync(c->staging(), uvw, 3 * rows * row, cudaMemcpyHostToDevice, c->stream));
-    k_spec_convert<float2, true><<<conv_blocks(tot), 256, 0, c->stream>>>(
-        (float2 *)c->slot_ptr(SLOT_SA), (double2 *)c->staging(), g, 3);
-    CKL();
-  }
-  CK(cudaStreamSynchronize(c->stream));
-  c->have_state = true;
-  return DNS_OK;
+  int st = set_spectral_view(c->grp, c->stream, uvw);
+  if (st == DNS_OK) c->have_state = true;
+  return st;
 }
 
 int dns_get_stale(dns_ctx *c, double *uvw) {
   if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  const long long nr = 3 * c->g.nreal;
-  if (c->precision == DNS_PREC_FP64) {
-    CK(cudaMemcpyAsync(uvw, c->stale, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  const Group &G = c->grp;
+  const long long nr = 3 * G.g.nreal;
+  if (G.precision == DNS_PREC_FP64) {
+    CK(cudaMemcpyAsync(uvw, G.stale, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   } else {
-    k_real_convert<float, double><<<conv_blocks(nr), 256, 0, c->stream>>>((const float *)c->stale, c->staging(), nr);
+    k_real_convert<float, double><<<conv_blocks(nr), 256, 0, c->stream>>>(
+        (const float *)G.stale, G.staging(0), nr);
     CKL();
-    CK(cudaMemcpyAsync(uvw, c->staging(), (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(uvw, G.staging(0), (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost,
                        c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -579,9 +667,9 @@ int dns_get_stale(dns_ctx *c, double *uvw) {
 
 int dns_set_stale(dns_ctx *c, const double *uvw) {
   if (!c || !uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  const long long nr = c->g.nreal;
+  const long long nr = c->grp.g.nreal;
   const double *src[3] = {uvw, uvw + nr, uvw + 2 * nr};
-  int st = upload_real3(c, src);
+  int st = upload_real3(c->grp, c->stream, src);
   if (st != DNS_OK) return st;
   CK(cudaStreamSynchronize(c->stream));
   return DNS_OK;
@@ -589,11 +677,11 @@ int dns_set_stale(dns_ctx *c, const double *uvw) {
 
 int dns_get_info(dns_ctx *c, dns_info_t *info) {
   if (!c || !info) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
-  info->n = c->n;
-  info->precision = c->precision;
-  info->flags = c->flags;
-  info->device_bytes = c->arena_bytes;
-  info->slot_bytes = (size_t)c->g.slot * c->csize;
+  info->n = c->grp.n;
+  info->precision = c->grp.precision;
+  info->flags = c->grp.flags;
+  info->device_bytes = c->grp.arena_bytes;
+  info->slot_bytes = (size_t)c->grp.g.slot * c->grp.csize;
   info->kernels_per_step = c->kernels_per_step;
   return DNS_OK;
 }
@@ -609,6 +697,12 @@ int dns_synchronize(dns_ctx *c) {
 int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) {
   if (!c || !ms || nsteps <= 0) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
   if (!c->have_state) return fail(DNS_ERR_STATE, "no velocity set", __FILE__, __LINE__);
+  if (!(nu == c->cur_nu && dt == c->cur_dt)) {
+    int st = set_coef(c->grp, c->stream, &nu, &dt);
+    if (st != DNS_OK) return st;
+    c->cur_nu = nu;
+    c->cur_dt = dt;
+  }
   const int K = c->kernels_per_step;
   std::vector<cudaEvent_t> ev(K + 1);
   for (auto &e : ev) CK(cudaEventCreate(&e));
@@ -617,8 +711,8 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
   for (long s = 0; s < nsteps && st == DNS_OK; s++) {
     CK(cudaEventRecord(ev[0], c->stream));
     for (int k = 0; k < K; k++) {
-      dispatch(c, [&](auto ops) {
-        decltype(ops)::stage_kernel(c, k / KERNELS_PER_STAGE, k % KERNELS_PER_STAGE, nu, dt);
+      dispatch(c->grp, [&](auto ops) {
+        decltype(ops)::stage_kernel(c->grp, c->stream, k / KERNELS_PER_STAGE, k % KERNELS_PER_STAGE);
       });
       CK(cudaEventRecord(ev[k + 1], c->stream));
     }
@@ -633,6 +727,180 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
   for (auto &e : ev) cudaEventDestroy(e);
   for (int k = 0; k < K; k++) ms[k] /= (double)nsteps;
   return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* ensemble                                                            */
+/* ------------------------------------------------------------------ */
+
+int dns_ens_destroy(dns_ens *e) {
+  if (!e) return DNS_OK;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (auto &G : e->groups) group_free(G);
+  for (auto s : e->gstreams) cudaStreamDestroy(s);
+  for (auto v : e->gevents) cudaEventDestroy(v);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->diag_host) cudaFreeHost(e->diag_host);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return DNS_OK;
+}
+
+int dns_ens_create(int nruns, const long *n, int precision, unsigned flags, dns_ens **out) {
+  if (!out || !n || nruns < 1) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  *out = nullptr;
+  dns_ens *e = new dns_ens();
+  e->nruns = nruns;
+  e->run_group.assign(nruns, -1);
+  e->run_index.assign(nruns, -1);
+  e->have_state.assign(nruns, 0);
+  std::vector<long> sizes;
+  for (int r = 0; r < nruns; r++) {
+    int gi = -1;
+    for (size_t q = 0; q < sizes.size(); q++)
+      if (sizes[q] == n[r]) gi = (int)q;
+    if (gi < 0) {
+      gi = (int)sizes.size();
+      sizes.push_back(n[r]);
+    }
+    e->run_group[r] = gi;
+  }
+  std::vector<int> counts(sizes.size(), 0);
+  for (int r = 0; r < nruns; r++) e->run_index[r] = counts[e->run_group[r]]++;
+  int st = DNS_OK;
+  cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaMallocHost((void **)&e->diag_host, sizeof(double4) * nruns);
+  if (ce != cudaSuccess) st = fail(DNS_ERR_CUDA, cudaGetErrorString(ce), __FILE__, __LINE__);
+  e->groups.resize(sizes.size());
+  for (size_t q = 0; q < sizes.size() && st == DNS_OK; q++) {
+    st = group_init(e->groups[q], sizes[q], precision, flags, counts[q], e->stream);
+    cudaStream_t gs = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (st == DNS_OK) {
+      ce = cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking);
+      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (ce != cudaSuccess) st = fail(DNS_ERR_CUDA, cudaGetErrorString(ce), __FILE__, __LINE__);
+      if (gs) e->gstreams.push_back(gs);
+      if (ev) e->gevents.push_back(ev);
+    }
+  }
+  if (st != DNS_OK) {
+    std::string keep = g_last_error;
+    dns_ens_destroy(e);
+    g_last_error = keep;
+    return st;
+  }
+  *out = e;
+  return DNS_OK;
+}
+
+static int ens_check_run(dns_ens *e, int run) {
+  if (!e || run < 0 || run >= e->nruns) return fail(DNS_ERR_ARG, "bad run index", __FILE__, __LINE__);
+  return DNS_OK;
+}
+
+int dns_ens_set_velocity(dns_ens *e, int run, const double *U, const double *V, const double *W) {
+  int st = ens_check_run(e, run);
+  if (st != DNS_OK) return st;
+  if (!U || !V || !W) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  const Group view = e->groups[e->run_group[run]].one(e->run_index[run]);
+  st = set_velocity_view(view, e->stream, U, V, W);
+  if (st == DNS_OK) e->have_state[run] = 1;
+  return st;
+}
+
+int dns_ens_set_params(dns_ens *e, const double *nu, const double *dt) {
+  if (!e || !nu || !dt) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  for (size_t q = 0; q < e->groups.size(); q++) {
+    const Group &G = e->groups[q];
+    std::vector<double> gn(G.nruns), gd(G.nruns);
+    for (int r = 0; r < e->nruns; r++)
+      if (e->run_group[r] == (int)q) gn[e->run_index[r]] = nu[r], gd[e->run_index[r]] = dt[r];
+    int st = set_coef(G, e->stream, gn.data(), gd.data());
+    if (st != DNS_OK) return st;
+  }
+  e->params_set = true;
+  return DNS_OK;
+}
+
+// one graph: a fork per size group (its own stream), each group's 24
+// batched kernels, then a join
+static int ens_build_graph(dns_ens *e) {
+  if (e->graph) return DNS_OK;
+  cudaGraph_t gr;
+  CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  cudaEventRecord(e->fork, e->stream);
+  for (size_t q = 0; q < e->groups.size(); q++) {
+    cudaStreamWaitEvent(e->gstreams[q], e->fork, 0);
+    const Group &G = e->groups[q];
+    dispatch(G, [&](auto ops) { decltype(ops)::step(G, e->gstreams[q]); });
+    cudaEventRecord(e->gevents[q], e->gstreams[q]);
+    cudaStreamWaitEvent(e->stream, e->gevents[q], 0);
+  }
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ce = cudaStreamEndCapture(e->stream, &gr);
+  if (le != cudaSuccess) return fail(DNS_ERR_CUDA, cudaGetErrorString(le), __FILE__, __LINE__);
+  CK(ce);
+  cudaError_t ie = cudaGraphInstantiate(&e->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  CK(ie);
+  return DNS_OK;
+}
+
+int dns_ens_step(dns_ens *e, long nsteps) {
+  if (!e || nsteps < 0) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  for (int r = 0; r < e->nruns; r++)
+    if (!e->have_state[r]) return fail(DNS_ERR_STATE, "a run has no velocity", __FILE__, __LINE__);
+  if (!e->params_set) return fail(DNS_ERR_STATE, "nu and dt not set", __FILE__, __LINE__);
+  if (nsteps == 0) return DNS_OK;
+  int st = ens_build_graph(e);
+  if (st != DNS_OK) return st;
+  for (long s = 0; s < nsteps; s++) CK(cudaGraphLaunch(e->graph, e->stream));
+  return DNS_OK;
+}
+
+int dns_ens_diagnostics(dns_ens *e, double *out) {
+  if (!e || !out) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  size_t base = 0;
+  std::vector<size_t> gbase(e->groups.size());
+  for (size_t q = 0; q < e->groups.size(); q++) {
+    const Group &G = e->groups[q];
+    dispatch(G, [&](auto ops) { decltype(ops)::diag(G, e->stream); });
+    CKL();
+    gbase[q] = base;
+    CK(cudaMemcpyAsync(e->diag_host + base, G.diag_out, sizeof(double4) * G.nruns,
+                       cudaMemcpyDeviceToHost, e->stream));
+    base += G.nruns;
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  bool finite = true;
+  for (int r = 0; r < e->nruns; r++) {
+    const double4 v = e->diag_host[gbase[e->run_group[r]] + e->run_index[r]];
+    out[4 * r + 0] = v.x;
+    out[4 * r + 1] = v.y;
+    out[4 * r + 2] = v.z;
+    out[4 * r + 3] = v.w;
+    finite = finite && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+  }
+  if (!finite) return fail(DNS_ERR_NONFINITE, "non-finite energy or enstrophy", __FILE__, __LINE__);
+  return DNS_OK;
+}
+
+int dns_ens_get_spectral(dns_ens *e, int run, double *uvw) {
+  int st = ens_check_run(e, run);
+  if (st != DNS_OK) return st;
+  if (!uvw) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
+  return get_spectral_view(e->groups[e->run_group[run]].one(e->run_index[run]), e->stream, uvw);
+}
+
+void *dns_ens_get_stream(dns_ens *e) { return e ? (void *)e->stream : nullptr; }
+
+int dns_ens_synchronize(dns_ens *e) {
+  if (!e) return fail(DNS_ERR_ARG, "NULL ensemble", __FILE__, __LINE__);
+  CK(cudaStreamSynchronize(e->stream));
+  return DNS_OK;
 }
 
 }  // extern "C"

@@ -42,15 +42,19 @@ struct Geo {
   int kcut;              // 2/3 rule: a wavenumber is kept iff |k| <= kcut
   long long slot;        // complex elements per spectral slot (n*n*nfp)
   long long nreal;       // n^3
+  long long run_spec;    // complex elements between two runs' slot sets
+  long long run_real;    // real elements between two runs' stale velocities
 };
 
 // A column pass processes tiles of W adjacent kz columns x the full line
-// along x or y.  Each block.z is one job: input slot -> output slot, and
-// optionally the derivative i*k*f (k along the pass axis) -> der slot.
+// along x or y.  block.z = job + njobs * run: each job maps an input slot to
+// an output slot and optionally the derivative i*k*f (k along the pass axis)
+// to a der slot, in every run of the batch.
 struct ColJobs {
   int in_slot[8];
   int out_slot[8];   // -1: no plain output
   int der_slot[8];   // -1: no derivative output
+  int njobs;
 };
 
 // column tile width: 128-byte tile rows
@@ -84,7 +88,7 @@ struct LineSync {
 
 // ---------------------------------------------------------------------------
 // Column pass along x (AXIS 0) or y (AXIS 1), forward or backward.
-// grid: (nfp / W, n, njobs); block: (N / E) * W threads.
+// grid: (nfp / W, n, njobs * nruns); block: (N / E) * W threads.
 // ---------------------------------------------------------------------------
 template <class R, int N, int AXIS, bool FWD>
 __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R>::W)
@@ -102,7 +106,10 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R>::W)
   const int col = blockIdx.x * W + p;
   const bool ok = col < g.nf;
   const int fixed = blockIdx.y;  // j for the x pass, i for the y pass
-  const int job = blockIdx.z;
+  const int job = blockIdx.z % jobs.njobs;
+  const long long rb = (long long)(blockIdx.z / jobs.njobs) * g.run_spec;
+  in += rb;
+  out += rb;
   long long base, rs;
   if (AXIS == 0) {
     base = (long long)fixed * g.nfp + col;
@@ -382,6 +389,8 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
   auto SU_ = [&](int f, int e) -> R & { return st[(f * E + e) * T + t]; };
   const long long line = (long long)blockIdx.x * Z::LINES + lid;
   const bool ok = line < (long long)N * N;
+  work += (long long)blockIdx.y * g.run_spec;  // run of the batch
+  stale += (long long)blockIdx.y * g.run_real;
   const long long off = line * g.nfp;
   const C *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
   const C *pW = work + SW * g.slot + off, *pDVDX = work + SDVDX * g.slot + off;
@@ -516,6 +525,9 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
 // A pure streaming kernel, one thread per half-spectrum point.  The
 // arithmetic is FP64 for both storage types (the FP32 path rounds on store).
 // ---------------------------------------------------------------------------
+// pointers are those of run 0; run r adds r * run_spec.  coef[2 r] = nu,
+// coef[2 r + 1] = dt of run r (device memory, so a captured graph picks up
+// new values without being rebuilt).
 template <class R>
 struct StageArgs {
   cx<R> *u0;    // step start state (3 slots); ST 3 writes the new state here
@@ -523,12 +535,14 @@ struct StageArgs {
   cx<R> *acc;   // RK accumulator (3 slots)
   cx<R> *next;  // next stage input (3 slots)
   cx<R> *ph;    // pressure slot or nullptr
-  double nu, dt, a, b;
+  const double *coef;
+  double a, b;  // RK coefficients of the stage (main.c:15-16)
 };
 
 template <class R, int ST>
 __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const Geo &g,
-                                             const StageArgs<R> &sa, long long q) {
+                                             const StageArgs<R> &sa, double nu, double dt,
+                                             long long q) {
   using C = cx<R>;
   const long long row = q / g.nf;
   const int col = (int)(q - row * g.nf);
@@ -538,7 +552,7 @@ __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const
   const double kx = (double)ikx, ky = (double)iky, kz = (double)col;
   const bool in = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
                   col <= g.kcut;
-  const double md = (double)in * sa.dt;
+  const double md = (double)in * dt;
   double2 du = cscale(to_d(nl[o]), md);
   double2 dv = cscale(to_d(nl[g.slot + o]), md);
   double2 dw = cscale(to_d(nl[2 * g.slot + o]), md);
@@ -550,7 +564,7 @@ __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const
   } else {
     P = make_double2(0.0, 0.0);
   }
-  const double c = sa.nu * sa.dt * kk;
+  const double c = nu * dt * kk;
   const double2 us0 = to_d(sa.us[o]), us1 = to_d(sa.us[g.slot + o]),
                 us2 = to_d(sa.us[2 * g.slot + o]);
   du = make_double2(du.x - (P.x * kx + c * us0.x), du.y - (P.y * kx + c * us0.y));
@@ -588,17 +602,31 @@ __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const
 }
 
 constexpr int UPD_THREADS = 256;
-constexpr int UPD_PER_THREAD = 2;
+// points per thread: enough bytes in flight per thread for either precision
+template <class R>
+struct UpdPer {
+  static constexpr int V = sizeof(R) == 8 ? 2 : 4;
+};
 
+// grid: (blocks per run, nruns)
 template <class R, int ST>
 __global__ void __launch_bounds__(UPD_THREADS)
     k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
+  constexpr int PER = UpdPer<R>::V;
+  const long long rb = (long long)blockIdx.y * g.run_spec;
+  nl += rb;
+  sa.u0 += rb;
+  sa.us += rb;
+  sa.acc += rb;
+  sa.next += rb;
+  if (sa.ph) sa.ph += rb;
+  const double nu = sa.coef[2 * blockIdx.y], dt = sa.coef[2 * blockIdx.y + 1];
   const long long npts = (long long)g.n * g.n * g.nf;
-  const long long q0 = (long long)blockIdx.x * UPD_THREADS * UPD_PER_THREAD + threadIdx.x;
+  const long long q0 = (long long)blockIdx.x * UPD_THREADS * PER + threadIdx.x;
 #pragma unroll
-  for (int u = 0; u < UPD_PER_THREAD; u++) {
+  for (int u = 0; u < PER; u++) {
     const long long q = q0 + (long long)u * UPD_THREADS;
-    if (q < npts) update_point<R, ST>(nl, g, sa, q);
+    if (q < npts) update_point<R, ST>(nl, g, sa, nu, dt, q);
   }
 }
 
@@ -660,9 +688,12 @@ __device__ __forceinline__ void dd_block_reduce(DD &e, DD &o, double4 *out) {
   }
 }
 
+// grid: (blocks per run, nruns); partials [run][gridDim.x]
 template <int BS, class C>
 __global__ void __launch_bounds__(BS)
     k_diag(const C *__restrict__ u, Geo g, double4 *__restrict__ partial) {
+  u += (long long)blockIdx.y * g.run_spec;
+  partial += (long long)blockIdx.y * gridDim.x;
   DD e{0.0, 0.0}, o{0.0, 0.0};
   const int n = g.n;
   const long long npts = (long long)n * n * g.nf;
@@ -682,9 +713,12 @@ __global__ void __launch_bounds__(BS)
   dd_block_reduce<BS>(e, o, partial + blockIdx.x);
 }
 
+// grid: (nruns); out[run]
 template <int BS>
 __global__ void __launch_bounds__(BS) k_diag_final(const double4 *__restrict__ partial, int np,
                                                    double4 *__restrict__ out) {
+  partial += (long long)blockIdx.x * np;
+  out += blockIdx.x;
   DD e{0.0, 0.0}, o{0.0, 0.0};
   for (int q = threadIdx.x; q < np; q += BS) {
     const double4 v = partial[q];

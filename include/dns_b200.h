@@ -132,6 +132,30 @@ int dns_synchronize(dns_ctx *ctx);
  * nsteps. */
 int dns_time_kernels(dns_ctx *ctx, double nu, double dt, long nsteps, double *ms);
 
+/* ---- ensemble: many independent runs stepped together ----
+ * No counterpart in the reference's main loop; it generalises its
+ * process-level ensembles (run.sh / hal.sh run one dns per core).  Runs of
+ * equal n share batched kernel launches; groups of different n run
+ * concurrently; one CUDA graph launch advances every run by one RK4 step.
+ * Each run follows main.c's step exactly (stale velocity included). */
+typedef struct dns_ens dns_ens;
+/* nruns runs, run r of grid size n[r] (same precision and flags for all) */
+int dns_ens_create(int nruns, const long *n, int precision, unsigned flags, dns_ens **out);
+int dns_ens_destroy(dns_ens *e);
+/* initial velocity of one run (as dns_set_velocity) */
+int dns_ens_set_velocity(dns_ens *e, int run, const double *U, const double *V, const double *W);
+/* viscosity and time step of every run (arrays of nruns) */
+int dns_ens_set_params(dns_ens *e, const double *nu, const double *dt);
+/* advance every run by nsteps RK4 steps */
+int dns_ens_step(dns_ens *e, long nsteps);
+/* per-run double-double sums as dns_diagnostics: out[4 r + 0..3] =
+ * e_hi, e_lo, om_hi, om_lo of run r */
+int dns_ens_diagnostics(dns_ens *e, double *out);
+/* spectral velocity of one run, layout of dns_get_spectral */
+int dns_ens_get_spectral(dns_ens *e, int run, double *uvw_hat);
+void *dns_ens_get_stream(dns_ens *e);
+int dns_ens_synchronize(dns_ens *e);
+
 /* Energy and enstrophy of a spectral velocity held in caller-owned device
  * memory, allocating nothing.  No counterpart in the reference (main.c has
  * no library interface); this is an addition for callers that may not call
