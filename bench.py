@@ -142,6 +142,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(ms: float, pg, device: str = "cuda") -> float:
+    """Slowest rank's time (every rank calls it at the same point)."""
+    if pg is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(steps: int, max_ms: float, world: int) -> float:
+    """Whole-job throughput of `world` independent replicas that each ran
+    `steps` steps, timed by the slowest one."""
+    return world * steps / (max_ms / 1000.0)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -336,12 +353,9 @@ def main() -> int:
     clk = clocks.stop()
     torch.cuda.synchronize()
     barrier()
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, pg)
     steps_per_s = args.steps / (ms / 1000.0)
-    value = steps_per_s * world
+    value = replica_rate(args.steps, ms, world)
 
     # -- per-kernel timing for the roofline --
     K = dns_b200.KERNELS_PER_STAGE
@@ -382,13 +396,11 @@ def main() -> int:
         cm.step(NU, DT, done64 - args.warmup - args.steps)
         E32, O32 = cm.diagnostics()
         mkms = cm.time_kernels(NU, DT, 2).reshape(4, K)
-    if pg is not None:
-        t = torch.tensor([mixed_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        mixed_ms = float(t.item())
+    mixed_ms = max_over_ranks(mixed_ms, pg)
     mixed_sps = args.steps / (mixed_ms / 1000.0)
     mixed = {
-        "value": mixed_sps * world, "unit": "steps/s", "ms_per_step": mixed_ms / args.steps,
+        "value": replica_rate(args.steps, mixed_ms, world), "unit": "steps/s",
+        "ms_per_step": mixed_ms / args.steps,
         "speedup_vs_fp64": mixed_sps / steps_per_s,
         "energy_rel_err_vs_fp64": float(abs(E32 - E64) / E64),
         "enstrophy_rel_err_vs_fp64": float(abs(O32 - O64) / O64),
@@ -430,11 +442,8 @@ def main() -> int:
         e1.synchronize()
         e2e_ms = e0.elapsed_time(e1)
         wall = time.perf_counter() - t0
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = args.steps / (e2e_ms / 1000.0) * world
+    e2e_ms = max_over_ranks(e2e_ms, pg)
+    e2e = replica_rate(args.steps, e2e_ms, world)
     h2d = 3 * n ** 3 * 8 / args.steps
     d2h = (3 * n ** 3 * 8 + 32 * ndiag) / args.steps
 
