@@ -84,6 +84,8 @@ _SIGS = {
     "dns_ens_get_spectral": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "dns_ens_get_stream": (_P, [_P]),
     "dns_ens_synchronize": (ctypes.c_int, [_P]),
+    "dns_adjoint_energy": (ctypes.c_int, [ctypes.c_long, _P, _P, _P, _D, _D, ctypes.c_long,
+                                          ctypes.c_int, _P, _P, _P, _P, _P]),
 }
 
 
@@ -314,6 +316,21 @@ def perturbed_tgv(n: int, seed: int, amplitude: float = 1e-3):
     d = solenoidal_perturbation(n, seed)
     s = amplitude * rms_tgv
     return U + s * d[0], V + s * d[1], W + s * d[2]
+
+
+def adjoint_energy(U, V, W, nu: float, dt: float, nsteps: int, snapshots: int = 20):
+    """Final energy J = E(T) (main.c's definition) after `nsteps` FP64 RK4
+    steps from (U, V, W), and its gradient: (J, (dJ/dU, dJ/dV, dJ/dW), dJ/dnu).
+    The adjoint runs on the GPU (dns_adjoint_energy)."""
+    lib = load_library()
+    U, V, W = _f64(U), _f64(V), _f64(W)
+    n = round(U.size ** (1.0 / 3))
+    g = [np.empty_like(U), np.empty_like(V), np.empty_like(W)]
+    J, gnu = ctypes.c_double(), ctypes.c_double()
+    _check(lib.dns_adjoint_energy(n, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, snapshots,
+                                  ctypes.byref(J), _ptr(g[0]), _ptr(g[1]), _ptr(g[2]),
+                                  ctypes.byref(gnu)))
+    return J.value, tuple(a.reshape(U.shape) for a in g), gnu.value
 
 
 def scale_diagnostics(eh, el, oh, ol, n):

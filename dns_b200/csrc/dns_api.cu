@@ -15,6 +15,7 @@
 // writes the new state back into SA, so the copies of main.c:334-342 and
 // main.c:415-420 disappear.
 #include "dns_b200.h"
+#include "adjoint.cuh"
 #include "kernels.cuh"
 
 #include <math.h>
@@ -189,6 +190,7 @@ ColJobs jobs_map(const int *in, const int *out, int cnt) {
 template <class R, int N>
 struct Ops {
   using C = cx<R>;
+  static constexpr int Nval = N;
   static constexpr int W = ColW<R>::W;
   static constexpr int E = Plan<N>::E;
   static constexpr int CT = (N / E) * W;
@@ -305,6 +307,40 @@ struct Ops {
     colpass<1, false>(G, st, jobs_map(w4, w4, nfields));
     k_zc2r<R, N><<<zgrid(nfields), ZCfg<N>::THREADS, Z_SMEM, st>>>(
         slot(G, SLOT_WORK), G.realbuf, tw(G), G.g, 1.0 / (double)G.g.nreal);
+  }
+
+  // c2r of K spectral fields (in + in_slots[f] * slot) into out[f * nreal],
+  // scaled (one run; uses the work slots)
+  static void c2r_fields(const Group &G, cudaStream_t st, const C *in, const int *in_slots, int K,
+                         double *out, double scale) {
+    C *wk = slot(G, SLOT_WORK);
+    ColJobs j1 = jobs_empty(K), j2 = jobs_empty(K);
+    for (int f = 0; f < K; f++) {
+      j1.in_slot[f] = in_slots[f];
+      j1.out_slot[f] = f;
+      j2.in_slot[f] = f;
+      j2.out_slot[f] = f;
+    }
+    dim3 grid(G.g.nfp / W, N, K);
+    k_colpass<R, N, 0, false><<<grid, CT, COL_SMEM, st>>>(in, wk, tw(G), G.g, j1);
+    k_colpass<R, N, 1, false><<<grid, CT, COL_SMEM, st>>>(wk, wk, tw(G), G.g, j2);
+    k_zc2r<R, N><<<zgrid(K), ZCfg<N>::THREADS, Z_SMEM, st>>>(wk, out, tw(G), G.g, scale);
+  }
+  // r2c of K real fields in[f * nreal] into spectral out + out_slots[f] * slot
+  static void r2c_fields(const Group &G, cudaStream_t st, const R *in, int K, C *out,
+                         const int *out_slots) {
+    C *wk = slot(G, SLOT_WORK);
+    ColJobs j1 = jobs_empty(K), j2 = jobs_empty(K);
+    for (int f = 0; f < K; f++) {
+      j1.in_slot[f] = f;
+      j1.out_slot[f] = out_slots[f];
+      j2.in_slot[f] = f;
+      j2.out_slot[f] = f;
+    }
+    k_zr2c<R, N><<<zgrid(K), ZCfg<N>::THREADS, Z_SMEM, st>>>(in, wk, tw(G), G.g);
+    dim3 grid(G.g.nfp / W, N, K);
+    k_colpass<R, N, 1, true><<<grid, CT, COL_SMEM, st>>>(wk, wk, tw(G), G.g, j2);
+    k_colpass<R, N, 0, true><<<grid, CT, COL_SMEM, st>>>(wk, out, tw(G), G.g, j1);
   }
 
   // energy / enstrophy sums of every run into diag_out[run]
@@ -509,6 +545,177 @@ int set_coef(const Group &G, cudaStream_t st, const double *nu, const double *dt
   CK(cudaMemcpyAsync(G.coef, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
   return DNS_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint of the RK4 step (FP64): gradient of the final energy
+// E(T) = invn3^2 sum_half |U_hat(T)|^2 (main.c:257-266's definition) with
+// respect to the initial velocity and nu.  Checkpoints of the step state
+// (U_hat, stale velocity) follow a binomial split of the step range.
+// ---------------------------------------------------------------------------
+// spectral work triples (in units of slots)
+enum { X_US0 = 0, X_LHAT = 12, X_LACC = 15, X_LDU = 18, X_LHAT0 = 21, X_LUS = 24, X_T1 = 27,
+       X_T2 = 30, NX = 33 };
+// real work triples (in units of n^3 fields)
+enum { RE_U = 0, RE_OM = 3, RE_LN = 6, RE_LU = 9, RE_LOM = 12, RE_LSTALE = 15, RE_STALEIN = 18,
+       NRE = 21 };
+
+struct Adj {
+  Group G;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  char *arena = nullptr;
+  cd *sp = nullptr;        // [NX][slot]
+  double *re = nullptr;    // [NRE][n^3]
+  cd *snap_sp = nullptr;   // [S][3][slot]
+  double *snap_re = nullptr;  // [S][3][n^3]
+  double4 *part = nullptr, *acc_nu = nullptr;
+  int nblocks = 0;
+  double nu = 0, dt = 0;
+  cd *X(int i) const { return sp + (size_t)i * G.g.slot; }
+  double *Rf(int i) const { return re + (size_t)i * G.g.nreal; }
+  size_t slot3() const { return (size_t)3 * G.g.slot * sizeof(cd); }
+  size_t real3() const { return (size_t)3 * G.g.nreal * sizeof(double); }
+};
+
+template <int N>
+struct AdjOps {
+  using O = Ops<double, N>;
+  static int copy3(Adj &A, void *dst, const void *src, size_t bytes) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, A.st));
+    return DNS_OK;
+  }
+  static unsigned pblocks(const Adj &A) { return (unsigned)A.nblocks; }
+
+  // adjoint of RK stage s: from lambda_dU (X_LDU) and U_s (X_US0 + 3 s)
+  // produce lambda_{U_s} (X_LUS); stage 0 also produces lambda_stale
+  static int stage(Adj &A, int s) {
+    const Group &G = A.G;
+    const Geo &g = G.g;
+    const double a = 1.0 / (double)g.nreal;
+    const int t3[3] = {0, 1, 2};
+    const cd *Us = A.X(X_US0 + 3 * s);
+    const double *u = A.Rf(RE_STALEIN);
+    if (s > 0) {
+      O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
+      u = A.Rf(RE_U);
+    }
+    const unsigned pb = pblocks(A);
+    k_curl<<<pb, 256, 0, A.st>>>(Us, A.X(X_T1), g);
+    O::c2r_fields(G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_OM), a);
+    k_adj_lamN<<<pb, 256, 0, A.st>>>(A.X(X_LDU), A.X(X_T1), g, A.dt);
+    O::c2r_fields(G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
+    k_adj_cross<<<conv_blocks(g.nreal), 256, 0, A.st>>>(
+        u, A.Rf(RE_OM), A.Rf(RE_LN), s == 3 ? A.Rf(RE_LSTALE) : nullptr, A.Rf(RE_LU),
+        A.Rf(RE_LOM), g.nreal);
+    O::r2c_fields(G, A.st, A.Rf(RE_LOM), 3, A.X(X_T1), t3);
+    if (s > 0) O::r2c_fields(G, A.st, A.Rf(RE_LU), 3, A.X(X_T2), t3);
+    k_adj_collect<256><<<pb, 256, 0, A.st>>>(A.X(X_T1), s > 0 ? A.X(X_T2) : nullptr, A.X(X_LDU), Us,
+                                             A.X(X_LUS), g, a, A.nu, A.dt, A.part);
+    k_dd_accumulate<256><<<1, 256, 0, A.st>>>(A.part, A.nblocks, A.acc_nu);
+    if (s == 0) {
+      int r = copy3(A, A.Rf(RE_LSTALE), A.Rf(RE_LU), A.real3());
+      if (r != DNS_OK) return r;
+    }
+    CKL();
+    return DNS_OK;
+  }
+
+  // adjoint of one step whose input state is in (SA, stale); lambda of the
+  // step output in (X_LHAT, RE_LSTALE) becomes lambda of its input
+  static int step(Adj &A) {
+    const Group &G = A.G;
+    const Geo &g = G.g;
+    const unsigned pb = pblocks(A);
+    int r;
+    if ((r = copy3(A, A.X(X_US0), G.slot_ptr(0, SLOT_SA), A.slot3()))) return r;
+    if ((r = copy3(A, A.Rf(RE_STALEIN), G.stale, A.real3()))) return r;
+    for (int s = 0; s < 4; s++) {  // forward again, keeping the stage inputs
+      for (int k = 0; k < KERNELS_PER_STAGE; k++) O::stage_kernel(G, A.st, s, k);
+      if (s < 3 && (r = copy3(A, A.X(X_US0 + 3 * (s + 1)), G.slot_ptr(0, SLOT_SB), A.slot3())))
+        return r;
+    }
+    if ((r = copy3(A, A.X(X_LACC), A.X(X_LHAT), A.slot3()))) return r;
+    if ((r = copy3(A, A.X(X_LHAT0), A.X(X_LHAT), A.slot3()))) return r;  // acc_0 = U0
+    for (int s = 3; s >= 0; s--) {
+      if (s == 3)
+        k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LACC), nullptr, A.X(X_LDU), g, RK_A[3], 0.0);
+      else  // U_{s+1} = U0 + b_s dU_s, acc += a_s dU_s
+        k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LUS), A.X(X_LACC), A.X(X_LDU), g, RK_B[s], RK_A[s]);
+      if ((r = stage(A, s))) return r;
+      // every stage input U_s is U0 plus a multiple of dU_{s-1}
+      k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LHAT0), A.X(X_LUS), A.X(X_LHAT0), g, 1.0, 1.0);
+    }
+    if ((r = copy3(A, A.X(X_LHAT), A.X(X_LHAT0), A.slot3()))) return r;
+    CKL();
+    return DNS_OK;
+  }
+};
+
+int adj_snap_store(Adj &A, int k) {
+  CK(cudaMemcpyAsync(A.snap_sp + (size_t)k * 3 * A.G.g.slot, A.G.slot_ptr(0, SLOT_SA), A.slot3(),
+                     cudaMemcpyDeviceToDevice, A.st));
+  CK(cudaMemcpyAsync(A.snap_re + (size_t)k * 3 * A.G.g.nreal, A.G.stale, A.real3(),
+                     cudaMemcpyDeviceToDevice, A.st));
+  return DNS_OK;
+}
+int adj_snap_restore(Adj &A, int k) {
+  CK(cudaMemcpyAsync(A.G.slot_ptr(0, SLOT_SA), A.snap_sp + (size_t)k * 3 * A.G.g.slot, A.slot3(),
+                     cudaMemcpyDeviceToDevice, A.st));
+  CK(cudaMemcpyAsync(A.G.stale, A.snap_re + (size_t)k * 3 * A.G.g.nreal, A.real3(),
+                     cudaMemcpyDeviceToDevice, A.st));
+  return DNS_OK;
+}
+int adj_advance(Adj &A, long m) {
+  for (long q = 0; q < m; q++) CK(cudaGraphLaunch(A.graph, A.st));
+  return DNS_OK;
+}
+int adj_step_one(Adj &A) {
+  int r = DNS_OK;
+  dispatch(A.G, [&](auto ops) {
+    using O = decltype(ops);
+    r = AdjOps<O::Nval>::step(A);
+  });
+  return r;
+}
+
+double binom(int n, int k) {
+  double r = 1.0;
+  for (int q = 1; q <= k; q++) r = r * (n - k + q) / q;
+  return r;
+}
+
+// reverse steps [a, b): the state at step a is in snapshot ka; snapshots
+// ka+1 .. ka+free are unused
+int adj_reverse(Adj &A, long a, long b, int ka, int free) {
+  int r;
+  if (b - a == 1) {
+    if ((r = adj_snap_restore(A, ka))) return r;
+    return adj_step_one(A);
+  }
+  if (free == 0) {  // no snapshot to spare: recompute from a for every step
+    for (long t = b - 1; t >= a; t--) {
+      if ((r = adj_snap_restore(A, ka))) return r;
+      if ((r = adj_advance(A, t - a))) return r;
+      if ((r = adj_step_one(A))) return r;
+    }
+    return DNS_OK;
+  }
+  // binomial split: smallest repetition number rr with C(free + rr, free)
+  // >= l; the right part gets what free - 1 snapshots reverse in rr
+  const long l = b - a;
+  int rr = 0;
+  while (binom(free + rr, free) < (double)l) rr++;
+  const double right_cap = binom(free - 1 + rr, free - 1);
+  long lr = right_cap < (double)(l - 1) ? (long)right_cap : l - 1;
+  if (lr < 1) lr = 1;
+  const long m = b - lr;
+  if ((r = adj_snap_restore(A, ka))) return r;
+  if ((r = adj_advance(A, m - a))) return r;
+  if ((r = adj_snap_store(A, ka + 1))) return r;
+  if ((r = adj_reverse(A, m, b, ka + 1, free - 1))) return r;
+  return adj_reverse(A, a, m, ka, free);
 }
 
 int ctx_build_graph(dns_ctx *c) {
@@ -901,6 +1108,113 @@ int dns_ens_synchronize(dns_ens *e) {
   if (!e) return fail(DNS_ERR_ARG, "NULL ensemble", __FILE__, __LINE__);
   CK(cudaStreamSynchronize(e->stream));
   return DNS_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* discrete adjoint                                                    */
+/* ------------------------------------------------------------------ */
+
+int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
+                       double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
+                       double *gW, double *gnu) {
+  if (!U || !V || !W || nsteps < 1 || snapshots < 1)
+    return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  Adj A;
+  CK(cudaStreamCreateWithFlags(&A.st, cudaStreamNonBlocking));
+  int r = group_init(A.G, n, DNS_PREC_FP64, 0, 1, A.st);
+  auto cleanup = [&]() {
+    if (A.st) cudaStreamSynchronize(A.st);
+    if (A.graph) cudaGraphExecDestroy(A.graph);
+    if (A.arena) cudaFree(A.arena);
+    group_free(A.G);
+    if (A.st) cudaStreamDestroy(A.st);
+  };
+  const Geo &g = A.G.g;
+  if (r == DNS_OK) r = set_coef(A.G, A.st, &nu, &dt);
+  A.nu = nu;
+  A.dt = dt;
+  A.nblocks = A.G.diag_blocks;
+  if (r == DNS_OK) {
+    const size_t sp_b = (size_t)NX * g.slot * sizeof(cd);
+    const size_t re_b = (size_t)NRE * g.nreal * sizeof(double);
+    const size_t ssp_b = (size_t)snapshots * 3 * g.slot * sizeof(cd);
+    const size_t sre_b = (size_t)snapshots * 3 * g.nreal * sizeof(double);
+    const size_t part_b = (size_t)(A.nblocks + 1) * sizeof(double4);
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    cudaError_t e = cudaMalloc((void **)&A.arena, al(sp_b) + al(re_b) + al(ssp_b) + al(sre_b) + al(part_b));
+    if (e != cudaSuccess) {
+      A.arena = nullptr;
+      r = fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
+    } else {
+      char *p = A.arena;
+      A.sp = (cd *)p; p += al(sp_b);
+      A.re = (double *)p; p += al(re_b);
+      A.snap_sp = (cd *)p; p += al(ssp_b);
+      A.snap_re = (double *)p; p += al(sre_b);
+      A.part = (double4 *)p;
+      A.acc_nu = A.part + A.nblocks;
+      e = cudaMemsetAsync(A.arena, 0, al(sp_b) + al(re_b), A.st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(A.acc_nu, 0, sizeof(double4), A.st);
+      if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+    }
+  }
+  if (r == DNS_OK) {  // graph of one forward step
+    cudaGraph_t gr;
+    cudaError_t e = cudaStreamBeginCapture(A.st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      dispatch(A.G, [&](auto ops) { decltype(ops)::step(A.G, A.st); });
+      e = cudaStreamEndCapture(A.st, &gr);
+      if (e == cudaSuccess) {
+        e = cudaGraphInstantiate(&A.graph, gr, 0);
+        cudaGraphDestroy(gr);
+      }
+    }
+    if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  if (r == DNS_OK) r = set_velocity_view(A.G, A.st, U, V, W);
+  if (r == DNS_OK) r = adj_snap_store(A, 0);
+  if (r == DNS_OK) r = adj_advance(A, nsteps);  // forward sweep to T
+  double4 d = make_double4(0, 0, 0, 0);
+  const double invn3 = 1.0 / (double)g.nreal;
+  if (r == DNS_OK) {
+    dispatch(A.G, [&](auto ops) { decltype(ops)::diag(A.G, A.st); });
+    cudaError_t e = cudaMemcpyAsync(&d, A.G.diag_out, sizeof(double4), cudaMemcpyDeviceToHost, A.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A.st);
+    if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  if (r == DNS_OK) {
+    // lambda(T) = dE/dU_hat = 2 invn3^2 U_hat(T); the stale velocity at T
+    // does not enter E
+    k_lincomb3<<<A.nblocks, 256, 0, A.st>>>((const cd *)A.G.slot_ptr(0, SLOT_SA), nullptr,
+                                            A.X(X_LHAT), g, 2.0 * invn3 * invn3, 0.0);
+    cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3(), A.st);
+    if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  if (r == DNS_OK) r = adj_reverse(A, 0, nsteps, 0, snapshots - 1);
+  if (r == DNS_OK) {
+    // dE/du0 = r2c^T(lambda_U(0)) + lambda_stale(0) = c2r(lambda / w_z) + lambda_stale
+    const int t3[3] = {0, 1, 2};
+    k_div_wz3<<<A.nblocks, 256, 0, A.st>>>(A.X(X_LHAT), A.X(X_T1), g);
+    dispatch(A.G, [&](auto ops) {
+      using O = decltype(ops);
+      Ops<double, O::Nval>::c2r_fields(A.G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
+    });
+    k_add_real<<<conv_blocks(3 * g.nreal), 256, 0, A.st>>>(A.Rf(RE_LSTALE), A.Rf(RE_LN), 3 * g.nreal);
+    cudaError_t e = cudaGetLastError();
+    double *dst[3] = {gU, gV, gW};
+    for (int f = 0; f < 3 && e == cudaSuccess; f++)
+      if (dst[f])
+        e = cudaMemcpyAsync(dst[f], A.Rf(RE_LN + f), (size_t)g.nreal * sizeof(double),
+                            cudaMemcpyDeviceToHost, A.st);
+    double4 gn = make_double4(0, 0, 0, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&gn, A.acc_nu, sizeof(double4), cudaMemcpyDeviceToHost, A.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(A.st);
+    if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+    if (J) *J = (d.x + d.y) * (invn3 * invn3);
+    if (gnu) *gnu = gn.x + gn.y;
+  }
+  cleanup();
+  return r;
 }
 
 }  // extern "C"

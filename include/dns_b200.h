@@ -156,6 +156,21 @@ int dns_ens_get_spectral(dns_ens *e, int run, double *uvw_hat);
 void *dns_ens_get_stream(dns_ens *e);
 int dns_ens_synchronize(dns_ens *e);
 
+/* ---- discrete adjoint ----
+ * No counterpart in the reference.  Gradient of the final energy
+ *   J = E(T) = invn3^2 * sum over the half spectrum of |U_hat(T)|^2
+ * (main.c:257-266's definition, no Hermitian weighting) after nsteps RK4
+ * steps of main.c's scheme (stale first-stage velocity included) from the
+ * initial velocity U, V, W (host, n^3 each), with respect to that initial
+ * velocity (gU, gV, gW: host, n^3 each, dJ/du0 at every grid point) and to
+ * nu (gnu).  FP64.  The transposed step is hand-written; forward states are
+ * recomputed from `snapshots` stored step states (>= 1, the initial state
+ * included) placed by a binomial split of the step range, so memory is
+ * independent of nsteps.  Any output pointer may be NULL. */
+int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
+                       double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
+                       double *gW, double *gnu);
+
 /* Energy and enstrophy of a spectral velocity held in caller-owned device
  * memory, allocating nothing.  No counterpart in the reference (main.c has
  * no library interface); this is an addition for callers that may not call

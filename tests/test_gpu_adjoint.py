@@ -1,0 +1,93 @@
+"""GPU tests of the discrete adjoint (dns_adjoint_energy): the gradient of
+the final energy with respect to the initial velocity and nu, against
+central finite differences of FP64 forward runs, along seeded directions.
+Tolerance 1e-6 relative (the target); the FD truncation and roundoff are
+~1e-9 here."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dns(dns_lib):
+    import dns_b200
+
+    return dns_b200
+
+
+def energy(dns, n, U, V, W, nu, dt, nsteps):
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        ctx.step(nu, dt, nsteps)
+        E, _ = ctx.diagnostics()
+    return E  # numpy longdouble
+
+
+def fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, directions, eps=1e-6, tol=1e-6):
+    for d in directions:
+        Jp = energy(dns, n, *(u0[c] + eps * d[c] for c in range(3)), nu, dt, nsteps)
+        Jm = energy(dns, n, *(u0[c] - eps * d[c] for c in range(3)), nu, dt, nsteps)
+        fd = float((Jp - Jm) / (2 * eps))
+        ad = float(sum(np.sum(g[c] * d[c]) for c in range(3)))
+        assert abs(fd - ad) <= tol * abs(ad), (fd, ad)
+    e = eps * nu
+    Jp = energy(dns, n, *u0, nu + e, dt, nsteps)
+    Jm = energy(dns, n, *u0, nu - e, dt, nsteps)
+    fd = float((Jp - Jm) / (2 * e))
+    assert abs(fd - gnu) <= tol * abs(gnu), (fd, gnu)
+
+
+def test_adjoint_matches_finite_differences_small(dns):
+    n, nu, dt, nsteps = 16, 0.02, 0.01, 12
+    u0 = dns.perturbed_tgv(n, seed=5, amplitude=0.3)
+    J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=4)
+    assert J == pytest.approx(float(energy(dns, n, *u0, nu, dt, nsteps)), rel=1e-14)
+    rng = np.random.default_rng(1)
+    dirs = [dns.solenoidal_perturbation(n, seed=s) for s in (11, 12)]
+    dirs.append([rng.standard_normal((n, n, n)) for _ in range(3)])  # not solenoidal
+    fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, dirs)
+
+
+def test_adjoint_independent_of_checkpointing(dns):
+    n, nu, dt, nsteps = 16, 0.01, 0.01, 9
+    u0 = dns.perturbed_tgv(n, seed=2, amplitude=0.2)
+    ref = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20)
+    for snaps in (1, 2, 3):
+        J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=snaps)
+        assert J == ref[0] and gnu == ref[2]
+        for c in range(3):
+            assert np.array_equal(g[c], ref[1][c])
+
+
+def test_adjoint_torch_autograd(dns):
+    import torch
+
+    from dns_b200.autograd import FinalEnergy
+
+    n, nu, dt, nsteps = 16, 0.02, 0.01, 5
+    u0 = torch.tensor(np.stack(dns.perturbed_tgv(n, seed=3, amplitude=0.3)), requires_grad=True)
+    nut = torch.tensor(nu, dtype=torch.float64, requires_grad=True)
+    J = FinalEnergy.apply(u0, nut, dt, nsteps, 3)
+    (3.0 * J).backward()
+    _, g, gnu = dns.adjoint_energy(*u0.detach().numpy(), nu, dt, nsteps, 3)
+    assert np.allclose(u0.grad.numpy(), 3.0 * np.stack(g), rtol=0, atol=0)
+    assert nut.grad.item() == 3.0 * gnu
+
+
+def test_adjoint_config_128(dns):
+    """Config: random isotropic solenoidal field, E(k) ~ k^4 exp(-2 (k/4)^2),
+    unit energy (main.c's half-spectrum E), 128^3, nu = 0.005, dt = 0.005,
+    T = 2 (401 steps by main.c's loop), 20 snapshots, 8 seeded directions."""
+    n, nu, dt = 128, 0.005, 0.005
+    _, nsteps = dns.step_schedule(2.0, dt)
+    assert nsteps == 401
+    u0 = dns.solenoidal_perturbation(n, seed=0)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(*u0)
+        E0, _ = ctx.diagnostics()
+    s = float(1.0 / np.sqrt(E0))
+    u0 = [c * s for c in u0]
+    J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20)
+    dirs = [dns.solenoidal_perturbation(n, seed=k) for k in range(1, 9)]
+    fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, dirs)
