@@ -191,10 +191,13 @@ template <class R, int N>
 struct Ops {
   using C = cx<R>;
   static constexpr int Nval = N;
-  static constexpr int W = ColW<R>::W;
   static constexpr int E = Plan<N>::E;
-  static constexpr int CT = (N / E) * W;
-  static constexpr size_t COL_SMEM = (size_t)(N + N * W) * sizeof(C);
+  template <int AXIS>
+  static constexpr int CW = ColW<R, AXIS, N>::W;
+  template <int AXIS>
+  static constexpr int CT = (N / E) * CW<AXIS>;
+  template <int AXIS>
+  static constexpr size_t COL_SMEM = (size_t)(N + N * CW<AXIS>) * sizeof(C);
   static constexpr size_t Z_SMEM = (size_t)(2 * N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(C);
   static constexpr size_t ZS_SMEM = ZC<R, N>::SMEM;
 
@@ -204,10 +207,10 @@ struct Ops {
   }
   static cudaError_t setup() {
     cudaError_t e;
-    if ((e = allow(k_colpass<R, N, 0, false>, COL_SMEM))) return e;
-    if ((e = allow(k_colpass<R, N, 0, true>, COL_SMEM))) return e;
-    if ((e = allow(k_colpass<R, N, 1, false>, COL_SMEM))) return e;
-    if ((e = allow(k_colpass<R, N, 1, true>, COL_SMEM))) return e;
+    if ((e = allow(k_colpass<R, N, 0, false>, COL_SMEM<0>))) return e;
+    if ((e = allow(k_colpass<R, N, 0, true>, COL_SMEM<0>))) return e;
+    if ((e = allow(k_colpass<R, N, 1, false>, COL_SMEM<1>))) return e;
+    if ((e = allow(k_colpass<R, N, 1, true>, COL_SMEM<1>))) return e;
     if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM))) return e;
     if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM))) return e;
     if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM))) return e;
@@ -220,9 +223,14 @@ struct Ops {
   static const C *tw(const Group &G) { return (const C *)G.tw; }
 
   template <int AXIS, bool FWD>
+  static void colpass_io(const Group &G, cudaStream_t st, const C *in, C *out, const ColJobs &jobs,
+                         int nruns) {
+    dim3 grid(G.g.nfp / CW<AXIS>, N, jobs.njobs * nruns);
+    k_colpass<R, N, AXIS, FWD><<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
+  }
+  template <int AXIS, bool FWD>
   static void colpass(const Group &G, cudaStream_t st, const ColJobs &jobs) {
-    dim3 grid(G.g.nfp / W, N, jobs.njobs * G.nruns);
-    k_colpass<R, N, AXIS, FWD><<<grid, CT, COL_SMEM, st>>>((C *)G.S, (C *)G.S, tw(G), G.g, jobs);
+    colpass_io<AXIS, FWD>(G, st, (C *)G.S, (C *)G.S, jobs, G.nruns);
   }
 
   static dim3 zgrid(int nfields) { return dim3((N * N) / ZCfg<N>::LINES, nfields); }
@@ -321,9 +329,8 @@ struct Ops {
       j2.in_slot[f] = f;
       j2.out_slot[f] = f;
     }
-    dim3 grid(G.g.nfp / W, N, K);
-    k_colpass<R, N, 0, false><<<grid, CT, COL_SMEM, st>>>(in, wk, tw(G), G.g, j1);
-    k_colpass<R, N, 1, false><<<grid, CT, COL_SMEM, st>>>(wk, wk, tw(G), G.g, j2);
+    colpass_io<0, false>(G, st, in, wk, j1, 1);
+    colpass_io<1, false>(G, st, wk, wk, j2, 1);
     k_zc2r<R, N><<<zgrid(K), ZCfg<N>::THREADS, Z_SMEM, st>>>(wk, out, tw(G), G.g, scale);
   }
   // r2c of K real fields in[f * nreal] into spectral out + out_slots[f] * slot
@@ -338,9 +345,8 @@ struct Ops {
       j2.out_slot[f] = f;
     }
     k_zr2c<R, N><<<zgrid(K), ZCfg<N>::THREADS, Z_SMEM, st>>>(in, wk, tw(G), G.g);
-    dim3 grid(G.g.nfp / W, N, K);
-    k_colpass<R, N, 1, true><<<grid, CT, COL_SMEM, st>>>(wk, wk, tw(G), G.g, j2);
-    k_colpass<R, N, 0, true><<<grid, CT, COL_SMEM, st>>>(wk, out, tw(G), G.g, j1);
+    colpass_io<1, true>(G, st, wk, wk, j2, 1);
+    colpass_io<0, true>(G, st, wk, out, j1, 1);
   }
 
   // energy / enstrophy sums of every run into diag_out[run]
@@ -416,7 +422,7 @@ int group_init(Group &G, long n, int precision, unsigned flags, int nruns, cudaS
   const bool fp64 = precision == DNS_PREC_FP64;
   G.csize = fp64 ? sizeof(double2) : sizeof(float2);
   G.rsize = fp64 ? sizeof(double) : sizeof(float);
-  const int W = fp64 ? ColW<double>::W : ColW<float>::W;
+  const int W = fp64 ? PitchW<double>::W : PitchW<float>::W;
   Geo &g = G.g;
   g.n = (int)n;
   g.nf = (int)(n / 2 + 1);

@@ -57,9 +57,18 @@ struct ColJobs {
   int njobs;
 };
 
-// column tile width: 128-byte tile rows
-template <class R>
+// column tile width: 128-byte tile rows (wider rows for the x passes, whose
+// rows lie a kx plane apart, measured slower: fewer, heavier blocks), capped
+// so that a block stays within 1024 threads
+template <class R, int AXIS, int N>
 struct ColW {
+  static constexpr int WB = 128 / (int)sizeof(cx<R>);
+  static constexpr int WT = 1024 / (N / Plan<N>::E);
+  static constexpr int W = WB < WT ? WB : WT;
+};
+// row pitch granularity (128 bytes): every tile width divides it
+template <class R>
+struct PitchW {
   static constexpr int W = 128 / (int)sizeof(cx<R>);
 };
 
@@ -88,14 +97,15 @@ struct LineSync {
 
 // ---------------------------------------------------------------------------
 // Column pass along x (AXIS 0) or y (AXIS 1), forward or backward.
-// grid: (nfp / W, n, njobs * nruns); block: (N / E) * W threads.
+// grid: (nfp / W, n, njobs * nruns); block: (N / E) * W threads
+// (W = ColW<R, AXIS, N>::W).
 // ---------------------------------------------------------------------------
 template <class R, int N, int AXIS, bool FWD>
-__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R>::W)
+__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
     k_colpass(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
               const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
   using C = cx<R>;
-  constexpr int W = ColW<R>::W;
+  constexpr int W = ColW<R, AXIS, N>::W;
   constexpr int E = Plan<N>::E, T = N / E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *st = (C *)smem_raw;  // stage twiddles (<= N entries)
@@ -119,32 +129,29 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R>::W)
     rs = g.nfp;
   }
   const C *src = in + (long long)jobs.in_slot[job] * g.slot + base;
-  C v[E];
-#pragma unroll
-  for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : czero<C>();
   const int oslot = jobs.out_slot[job], dslot = jobs.der_slot[job];
-  C d[E];
-  if (dslot >= 0) {
+  C v[E];
+  // the input is read twice (the second read is an L2 hit) rather than kept
+  // in a second register array: first for the derivative i k f, then for the
+  // plain transform, which may overwrite the input in place
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R k = (R)kwave(t + T * e, N);
-      d[e] = cmk<C>(-k * v[e].y, k * v[e].x);  // i k f
+  for (int pass = 0; pass < 2; pass++) {
+    const int dst_slot = pass == 0 ? dslot : oslot;
+    if (dst_slot < 0) continue;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : czero<C>();
+    if (pass == 0) {
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const R k = (R)kwave(t + T * e, N);
+        v[e] = cmk<C>(-k * v[e].y, k * v[e].x);  // i k f
+      }
     }
-  }
-  if (oslot >= 0) {
     line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, BlockSync{});
     if (ok) {
-      C *dst = out + (long long)oslot * g.slot + base;
+      C *dst = out + (long long)dst_slot * g.slot + base;
 #pragma unroll
       for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = v[e];
-    }
-  }
-  if (dslot >= 0) {
-    line_fft<N, Plan<N>, FWD>(d, t, st, xb, ColIdx<W>{p}, BlockSync{});
-    if (ok) {
-      C *dst = out + (long long)dslot * g.slot + base;
-#pragma unroll
-      for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = d[e];
     }
   }
 }
