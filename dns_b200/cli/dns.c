@@ -12,6 +12,10 @@
  * The -v lines report the CUDA device instead of the OpenMP thread count.
  * A NaN/Inf in the diagnostics ends the run with an error message and exit
  * status 1 (the reference dies on SIGFPE, main.c:49-50).
+ *
+ * The environment variable DNS_B200_PRECISION selects the arithmetic
+ * without touching the reference's flags: "fp64" (default, the reference's)
+ * or "mixed" (float32 fields and FFTs, float64 reductions).
  */
 #define _GNU_SOURCE
 #include <fenv.h>
@@ -207,8 +211,18 @@ int main(int argc, char **argv) {
     exit(1);
   }
 
+  int prec = DNS_PREC_FP64;
+  const char *penv = getenv("DNS_B200_PRECISION");
+  if (penv != NULL && *penv != '\0') {
+    if (strcmp(penv, "mixed") == 0)
+      prec = DNS_PREC_MIXED;
+    else if (strcmp(penv, "fp64") != 0) {
+      fprintf(stderr, "dns: error: DNS_B200_PRECISION='%s' is not fp64 or mixed\n", penv);
+      exit(1);
+    }
+  }
   dns_ctx *ctx;
-  int st = dns_create(n, DNS_PREC_FP64, dump ? DNS_FLAG_PRESSURE : 0u, &ctx);
+  int st = dns_create(n, prec, dump ? DNS_FLAG_PRESSURE : 0u, &ctx);
   if (st != DNS_OK)
     die_status("dns_create", st);
   if (verbose) {

@@ -263,3 +263,25 @@ def test_cli_dump_matches_reference(dns, oracle_lib, tmp_path):
             fa = np.frombuffer(a).reshape(4, n, n, n)
             fb = np.frombuffer(b).reshape(4, n, n, n)
             assert rel_l2(fa[:3], fb[:3]) <= ROUND_TOL
+
+
+def test_cli_mixed_precision_env(dns, tmp_path):
+    """DNS_B200_PRECISION=mixed runs the float32 path behind the same CLI:
+    same line format and step count, energy within 1e-5 of the reference."""
+    import os
+
+    raw = str(tmp_path / "tgv.raw")
+    dns.write_raw(raw, dns.tgv_fields(32))
+    env = dict(os.environ, DNS_B200_PRECISION="mixed")
+    r = subprocess.run([dns.CLI_PATH, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", "0.2"],
+                       capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stderr
+    got = r.stdout.splitlines()
+    want = open(os.path.join(GOLDEN, "refrun_tgv32_nu0.01_dt0.01_T0.2.txt")).read().splitlines()
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        assert g[:34] == w[:34] and len(g) == len(w)
+        assert abs(float(g.split()[2]) - float(w.split()[2])) <= 1e-5 * float(w.split()[2])
+    bad = subprocess.run([dns.CLI_PATH, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", "0.2"],
+                         capture_output=True, text=True, env=dict(os.environ, DNS_B200_PRECISION="fp16"))
+    assert bad.returncode == 1 and "DNS_B200_PRECISION" in bad.stderr
