@@ -171,16 +171,49 @@ def _golden_run(dns, n, re_, nlines):
 @pytest.mark.parametrize("re_", ["0100", "0200", "0400", "0800", "1600", "3000"])
 def test_golden_0128_t1(dns, re_):
     """128^3 Taylor-Green against the reference's FFTW history over t in
-    [0, 1] (400 steps, 41 printed lines)."""
+    [0, 1] (400 steps, 41 printed lines).
+
+    The published 0128 histories follow main.c only up to t ~ 0.9: after
+    that they depart from main.c restated (the oracle) by a difference that
+    doubles every ~10 steps at every Re and that does not depend on the
+    dealiasing mask; the same departure separates them from the published
+    0256 histories.  The GPU path and the oracle stay within 1e-16 of each
+    other past that point (test_oracle_0128_t2), and the 256^3 histories
+    are matched over the whole run (test_golden_0256_full)."""
     de, do = _golden_run(dns, 128, re_, 41)
     assert de.max() <= E_TOL and do.max() <= E_TOL, (float(de.max()), float(do.max()))
 
 
-@pytest.mark.parametrize("re_", ["1600", "3000"])
-def test_golden_0256_t1(dns, re_):
-    """256^3 Taylor-Green against the reference's FFTW history, t in [0, 1]."""
-    de, do = _golden_run(dns, 256, re_, 41)
-    assert de.max() <= E_TOL and do.max() <= E_TOL, (float(de.max()), float(do.max()))
+@pytest.mark.parametrize("re_", ["0100", "1600", "3000"])
+def test_golden_0256_full(dns, re_):
+    """256^3 Taylor-Green against the reference's FFTW history over the
+    whole published run, t in [0, 10] (4000 steps, 401 printed lines)."""
+    de, do = _golden_run(dns, 256, re_, 401)
+    assert de.max() <= 1e-13 and do.max() <= 1e-13, (float(de.max()), float(do.max()))
+
+
+def test_oracle_0128_t2(dns, oracle_lib):
+    """128^3 Taylor-Green at Re = 3000 against main.c restated, over t in
+    [0, 2] (800 steps): the window where the published 0128 histories no
+    longer follow main.c."""
+    oracle_lib.set_threads(min(16, os.cpu_count() or 1))
+    n, nu, dt = 128, float("%.16e" % (1.0 / 3000)), 0.0025
+    U, V, W, _ = dns.tgv_fields(n)
+    o = oracle_lib.Oracle(n)
+    o.set_velocity(U, V, W)
+    worst = 0.0
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        for q in range(81):
+            if q:
+                ctx.step(nu, dt, 10)
+                o.step(nu, dt, 10)
+            e, w = ctx.diagnostics()
+            eo, wo = o.diagnostics()
+            worst = max(worst, float(abs(e - eo) / eo), float(abs(w - wo) / wo))
+    o.close()
+    oracle_lib.set_threads(min(4, os.cpu_count() or 1))
+    assert worst <= 1e-13, worst
 
 
 # ---------------------------------------------------------------- errors
