@@ -316,9 +316,11 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 //        z axis being the last, real one); Re y = a, Im y = b.
 //   r2c: Y = a + i b; X_a[k] = (Z[k] + conj Z[N-k]) / 2,
 //        X_b[k] = -i (Z[k] - conj Z[N-k]) / 2.
-// T = N/E threads per line hold E points each; the velocity and two of the
-// u x omega partial sums are staged in shared memory (each thread only reads
-// back its own points).
+// T = N/E threads per line hold E points each.  In the middle stages the
+// pairs (u, omega_y), (w, omega_z), (v, omega_x) read each input slot once
+// and u x omega accumulates in registers; the first and last stages stage
+// the velocity and two partial sums in shared memory (each thread only
+// reads back its own points).
 // KIND 0: first stage, velocity from the stale real slots (main.c:344 skips
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
@@ -364,6 +366,34 @@ __device__ __forceinline__ void ext_pair(C (&y)[ZC<R, N>::E], int t, FA fa, FB f
       const bool direct = k <= Z::M;
       const int s = direct ? k : N - k;
       C a = fa(s), b = fb(s);
+      if (s == 0 || s == Z::M) {
+        a.y = 0;
+        b.y = 0;
+      }
+      if (!direct) {
+        a.y = -a.y;
+        b.y = -b.y;
+      }
+      y[e] = cmk<C>(a.x - b.y, a.y + b.x);
+    }
+    asm volatile("" ::: "memory");
+  }
+}
+
+// Same, with one functor giving both spectra at a position, so that a field
+// feeding both halves (u for u and omega_y) is loaded once.
+template <class R, int N, int CH = 4, class C, class FAB>
+__device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N>::E], int t, FAB fab) {
+  using Z = ZC<R, N>;
+#pragma unroll
+  for (int e0 = 0; e0 < Z::E; e0 += CH) {
+#pragma unroll
+    for (int e = e0; e < e0 + CH && e < Z::E; e++) {
+      const int k = t + Z::T * e;
+      const bool direct = k <= Z::M;
+      const int s = direct ? k : N - k;
+      C a, b;
+      fab(s, a, b);
       if (s == 0 || s == Z::M) {
         a.y = 0;
         b.y = 0;
@@ -448,7 +478,54 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       nx[e] += SU_(1, e) * oz;
       ny[e] -= SU_(0, e) * oz;
     }
+  } else if (KIND == 1) {
+    // Pairs ordered so that every input slot is read once and the cross
+    // product accumulates in registers:
+    //   (u, omega_y): N_z = u oy
+    //   (w, omega_z): N_x = -w oy, N_y = -u oz
+    //   (v, omega_x): N_x += v oz, N_y += w ox, N_z -= v ox
+    R u[E], oy[E];
+    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+      const C uu = ld(pU, s), d = ld(pDWDX, s);
+      a = uu;
+      b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      u[e] = y[e].x * invn3;
+      oy[e] = y[e].y * invn3;
+      nz[e] = u[e] * oy[e];
+    }
+    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+      a = ld(pW, s);
+      b = csub(ld(pDVDX, s), ld(pDUDY, s));  // dv/dx - du/dy
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+    R w[E], oz[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      w[e] = y[e].x * invn3;
+      oz[e] = y[e].y * invn3;
+      nx[e] = -w[e] * oy[e];
+      ny[e] = -u[e] * oz[e];
+    }
+    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+      const C vv = ld(pV, s), d = ld(pDWDY, s);
+      a = vv;
+      b = cmk<C>(d.x + (R)s * vv.y, d.y - (R)s * vv.x);  // dw/dy - i kz v
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R v = y[e].x * invn3, ox = y[e].y * invn3;
+      nx[e] += v * oz[e];
+      ny[e] += w[e] * ox;
+      nz[e] -= v * ox;
+    }
   } else {
+    // last stage: the velocity is also stored as the next stale one, so it
+    // is staged in shared memory (the register-only order above spills here)
     // (u, v)
     ext_pair<R, N>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
