@@ -279,14 +279,14 @@ struct Ops {
         sa.coef = G.coef;
         sa.a = RK_A[s];
         sa.b = s < 3 ? RK_B[s] : 0.0;
-        const long long npts = (long long)N * N * g.nf;
+        const long long npad = (long long)N * N * g.nfp;
         const int per = UPD_THREADS * UpdPer<R>::V;
-        dim3 grid((unsigned)((npts + per - 1) / per), G.nruns);
+        dim3 grid((unsigned)((npad + per - 1) / per), G.nruns);
         switch (s) {
-          case 0: k_update<R, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          case 1: k_update<R, 1><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          case 2: k_update<R, 2><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          default: k_update<R, 3><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          case 0: k_update<R, N, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          case 1: k_update<R, N, 1><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          case 2: k_update<R, N, 2><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
+          default: k_update<R, N, 3><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
         }
       }
     }

@@ -626,12 +626,8 @@ struct StageArgs {
 template <class R, int ST>
 __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const Geo &g,
                                              const StageArgs<R> &sa, double nu, double dt,
-                                             long long q) {
+                                             long long o, int i, int j, int col) {
   using C = cx<R>;
-  const long long row = q / g.nf;
-  const int col = (int)(q - row * g.nf);
-  const int i = (int)(row / g.n), j = (int)(row - (long long)i * g.n);
-  const long long o = row * g.nfp + col;
   const int ikx = kwave(i, g.n), iky = kwave(j, g.n);
   const double kx = (double)ikx, ky = (double)iky, kz = (double)col;
   const bool in = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
@@ -692,11 +688,16 @@ struct UpdPer {
   static constexpr int V = sizeof(R) == 8 ? 2 : 4;
 };
 
-// grid: (blocks per run, nruns)
-template <class R, int ST>
+// grid: (blocks per run, nruns).  The points are walked in slot order,
+// padding columns included (and skipped), so that the row, kx and ky of a
+// point come from divisions by compile-time constants.
+template <class R, int N, int ST>
 __global__ void __launch_bounds__(UPD_THREADS)
     k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
   constexpr int PER = UpdPer<R>::V;
+  constexpr int NF = N / 2 + 1;
+  constexpr int NFP = (NF + PitchW<R>::W - 1) / PitchW<R>::W * PitchW<R>::W;
+  constexpr unsigned NPAD = (unsigned)N * N * NFP;
   const long long rb = (long long)blockIdx.y * g.run_spec;
   nl += rb;
   sa.u0 += rb;
@@ -705,12 +706,14 @@ __global__ void __launch_bounds__(UPD_THREADS)
   sa.next += rb;
   if (sa.ph) sa.ph += rb;
   const double nu = sa.coef[2 * blockIdx.y], dt = sa.coef[2 * blockIdx.y + 1];
-  const long long npts = (long long)g.n * g.n * g.nf;
-  const long long q0 = (long long)blockIdx.x * UPD_THREADS * PER + threadIdx.x;
+  const unsigned q0 = blockIdx.x * (unsigned)(UPD_THREADS * PER) + threadIdx.x;
 #pragma unroll
   for (int u = 0; u < PER; u++) {
-    const long long q = q0 + (long long)u * UPD_THREADS;
-    if (q < npts) update_point<R, ST>(nl, g, sa, nu, dt, q);
+    const unsigned q = q0 + (unsigned)u * UPD_THREADS;
+    const unsigned row = q / NFP;
+    const int col = (int)(q - row * NFP);
+    if (q < NPAD && col < NF)
+      update_point<R, ST>(nl, g, sa, nu, dt, (long long)q, (int)(row / N), (int)(row % N), col);
   }
 }
 
