@@ -280,7 +280,7 @@ struct Ops {
         sa.a = RK_A[s];
         sa.b = s < 3 ? RK_B[s] : 0.0;
         const long long npad = (long long)N * N * g.nfp;
-        const int per = UPD_THREADS * UpdPer<R>::V;
+        const int per = UPD_THREADS * UpdVec<R>::VP;
         dim3 grid((unsigned)((npad + per - 1) / per), G.nruns);
         switch (s) {
           case 0: k_update<R, N, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;

@@ -623,19 +623,36 @@ struct StageArgs {
   double a, b;  // RK coefficients of the stage (main.c:15-16)
 };
 
+// Inputs and results of one point.  A thread loads every input of its
+// points before the first store: as far as the compiler knows the stores may
+// alias later inputs, which would otherwise hold loads back behind them.
+template <class R>
+struct UpdIn {
+  cx<R> n[3];   // N slots (E1 output)
+  cx<R> us[3];  // stage input
+  cx<R> z[3];   // u0 (ST 1, 2)
+  cx<R> a[3];   // accumulator (ST 1, 2, 3)
+};
+template <class R>
+struct UpdOut {
+  cx<R> o1[3];  // next stage input (ST 0-2) or the new state (ST 3)
+  cx<R> o2[3];  // accumulator (ST 0-2)
+  cx<R> p;      // pressure
+};
+
 template <class R, int ST>
-__device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const Geo &g,
-                                             const StageArgs<R> &sa, double nu, double dt,
-                                             long long o, int i, int j, int col) {
+__device__ __forceinline__ void update_point(const UpdIn<R> &in, UpdOut<R> &out, const Geo &g,
+                                             const StageArgs<R> &sa, double nu, double dt, int i,
+                                             int j, int col) {
   using C = cx<R>;
   const int ikx = kwave(i, g.n), iky = kwave(j, g.n);
   const double kx = (double)ikx, ky = (double)iky, kz = (double)col;
-  const bool in = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
-                  col <= g.kcut;
-  const double md = (double)in * dt;
-  double2 du = cscale(to_d(nl[o]), md);
-  double2 dv = cscale(to_d(nl[g.slot + o]), md);
-  double2 dw = cscale(to_d(nl[2 * g.slot + o]), md);
+  const bool inm = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
+                   col <= g.kcut;
+  const double md = (double)inm * dt;
+  double2 du = cscale(to_d(in.n[0]), md);
+  double2 dv = cscale(to_d(in.n[1]), md);
+  double2 dw = cscale(to_d(in.n[2]), md);
   const double kk = kx * kx + ky * ky + kz * kz;
   double2 P;
   if (kk > 0) {
@@ -645,75 +662,124 @@ __device__ __forceinline__ void update_point(const cx<R> *__restrict__ nl, const
     P = make_double2(0.0, 0.0);
   }
   const double c = nu * dt * kk;
-  const double2 us0 = to_d(sa.us[o]), us1 = to_d(sa.us[g.slot + o]),
-                us2 = to_d(sa.us[2 * g.slot + o]);
+  const double2 us0 = to_d(in.us[0]), us1 = to_d(in.us[1]), us2 = to_d(in.us[2]);
   du = make_double2(du.x - (P.x * kx + c * us0.x), du.y - (P.y * kx + c * us0.y));
   dv = make_double2(dv.x - (P.x * ky + c * us1.x), dv.y - (P.y * ky + c * us1.y));
   dw = make_double2(dw.x - (P.x * kz + c * us2.x), dw.y - (P.y * kz + c * us2.y));
-  if (sa.ph) sa.ph[o] = from_d<C>(P);
+  out.p = from_d<C>(P);
   auto axpy = [](double2 x, double s, double2 y) {
     return make_double2(x.x + s * y.x, x.y + s * y.y);
   };
-  if (ST == 0) {  // us == u0
-    sa.next[o] = from_d<C>(axpy(us0, sa.b, du));
-    sa.next[g.slot + o] = from_d<C>(axpy(us1, sa.b, dv));
-    sa.next[2 * g.slot + o] = from_d<C>(axpy(us2, sa.b, dw));
-    sa.acc[o] = from_d<C>(axpy(us0, sa.a, du));
-    sa.acc[g.slot + o] = from_d<C>(axpy(us1, sa.a, dv));
-    sa.acc[2 * g.slot + o] = from_d<C>(axpy(us2, sa.a, dw));
-  } else if (ST < 3) {
-    const double2 z0 = to_d(sa.u0[o]), z1 = to_d(sa.u0[g.slot + o]),
-                  z2 = to_d(sa.u0[2 * g.slot + o]);
-    const double2 a0 = to_d(sa.acc[o]), a1 = to_d(sa.acc[g.slot + o]),
-                  a2 = to_d(sa.acc[2 * g.slot + o]);
-    sa.next[o] = from_d<C>(axpy(z0, sa.b, du));
-    sa.next[g.slot + o] = from_d<C>(axpy(z1, sa.b, dv));
-    sa.next[2 * g.slot + o] = from_d<C>(axpy(z2, sa.b, dw));
-    sa.acc[o] = from_d<C>(axpy(a0, sa.a, du));
-    sa.acc[g.slot + o] = from_d<C>(axpy(a1, sa.a, dv));
-    sa.acc[2 * g.slot + o] = from_d<C>(axpy(a2, sa.a, dw));
-  } else {
-    const double2 a0 = to_d(sa.acc[o]), a1 = to_d(sa.acc[g.slot + o]),
-                  a2 = to_d(sa.acc[2 * g.slot + o]);
-    sa.u0[o] = from_d<C>(axpy(a0, sa.a, du));
-    sa.u0[g.slot + o] = from_d<C>(axpy(a1, sa.a, dv));
-    sa.u0[2 * g.slot + o] = from_d<C>(axpy(a2, sa.a, dw));
+  const double2 d[3] = {du, dv, dw};
+#pragma unroll
+  for (int f = 0; f < 3; f++) {
+    if (ST == 0) {  // us == u0
+      const double2 u = to_d(in.us[f]);
+      out.o1[f] = from_d<C>(axpy(u, sa.b, d[f]));
+      out.o2[f] = from_d<C>(axpy(u, sa.a, d[f]));
+    } else if (ST < 3) {
+      out.o1[f] = from_d<C>(axpy(to_d(in.z[f]), sa.b, d[f]));
+      out.o2[f] = from_d<C>(axpy(to_d(in.a[f]), sa.a, d[f]));
+    } else {
+      out.o1[f] = from_d<C>(axpy(to_d(in.a[f]), sa.a, d[f]));
+    }
   }
 }
 
 constexpr int UPD_THREADS = 256;
-// points per thread: enough bytes in flight per thread for either precision
+// adjacent points per vector access: two float2 make one 16-byte access
 template <class R>
-struct UpdPer {
-  static constexpr int V = sizeof(R) == 8 ? 2 : 4;
+struct UpdVec;
+template <>
+struct UpdVec<double> {
+  static constexpr int VP = 1;
+  using T = double2;
+  __device__ static double2 get(const T &v, int) { return v; }
+  __device__ static T pack(const double2 *c) { return c[0]; }
+};
+template <>
+struct UpdVec<float> {
+  static constexpr int VP = 2;
+  using T = float4;
+  __device__ static float2 get(const T &v, int k) {
+    return k ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+  }
+  __device__ static T pack(const float2 *c) { return make_float4(c[0].x, c[0].y, c[1].x, c[1].y); }
 };
 
-// grid: (blocks per run, nruns).  The points are walked in slot order,
-// padding columns included (and skipped), so that the row, kx and ky of a
-// point come from divisions by compile-time constants.
+// grid: (ceil(n^2 nfp / VP / UPD_THREADS), nruns).  Thread = VP adjacent
+// points of the padded slot (padding columns included and skipped), so that
+// the row, kx and ky of a point come from divisions by compile-time constants.
 template <class R, int N, int ST>
 __global__ void __launch_bounds__(UPD_THREADS)
     k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
-  constexpr int PER = UpdPer<R>::V;
+  using VT = UpdVec<R>;
+  using V = typename VT::T;
+  constexpr int VP = VT::VP;
   constexpr int NF = N / 2 + 1;
   constexpr int NFP = (NF + PitchW<R>::W - 1) / PitchW<R>::W * PitchW<R>::W;
   constexpr unsigned NPAD = (unsigned)N * N * NFP;
+  static_assert(NFP % VP == 0, "vector access must not straddle rows");
+  const unsigned q0 = (blockIdx.x * (unsigned)UPD_THREADS + threadIdx.x) * VP;
+  if (q0 >= NPAD) return;
+  const unsigned row = q0 / NFP;
+  const int col0 = (int)(q0 - row * NFP);
+  if (col0 >= NF) return;
   const long long rb = (long long)blockIdx.y * g.run_spec;
-  nl += rb;
-  sa.u0 += rb;
-  sa.us += rb;
-  sa.acc += rb;
-  sa.next += rb;
-  if (sa.ph) sa.ph += rb;
   const double nu = sa.coef[2 * blockIdx.y], dt = sa.coef[2 * blockIdx.y + 1];
-  const unsigned q0 = blockIdx.x * (unsigned)(UPD_THREADS * PER) + threadIdx.x;
+  const long long vo = (rb + q0) / VP, vs = g.slot / VP;  // vector index, slot stride
+  const V *vn = (const V *)nl, *vus = (const V *)sa.us, *vz = (const V *)sa.u0,
+          *va = (const V *)sa.acc;
+  V ln[3], lus[3], lz[3], la[3];
 #pragma unroll
-  for (int u = 0; u < PER; u++) {
-    const unsigned q = q0 + (unsigned)u * UPD_THREADS;
-    const unsigned row = q / NFP;
-    const int col = (int)(q - row * NFP);
-    if (q < NPAD && col < NF)
-      update_point<R, ST>(nl, g, sa, nu, dt, (long long)q, (int)(row / N), (int)(row % N), col);
+  for (int f = 0; f < 3; f++) {
+    ln[f] = vn[f * vs + vo];
+    lus[f] = vus[f * vs + vo];
+    if (ST == 1 || ST == 2) lz[f] = vz[f * vs + vo];
+    if (ST != 0) la[f] = va[f * vs + vo];
+  }
+  UpdOut<R> res[VP];
+#pragma unroll
+  for (int v = 0; v < VP; v++) {
+    if (col0 + v < NF) {
+      UpdIn<R> in;
+#pragma unroll
+      for (int f = 0; f < 3; f++) {
+        in.n[f] = VT::get(ln[f], v);
+        in.us[f] = VT::get(lus[f], v);
+        if (ST == 1 || ST == 2) in.z[f] = VT::get(lz[f], v);
+        if (ST != 0) in.a[f] = VT::get(la[f], v);
+      }
+      update_point<R, ST>(in, res[v], g, sa, nu, dt, (int)(row / N), (int)(row % N), col0 + v);
+    }
+  }
+  V *o1 = (V *)(ST == 3 ? sa.u0 : sa.next), *o2 = (V *)sa.acc, *vp = (V *)sa.ph;
+  if (col0 + VP - 1 < NF) {
+    cx<R> t1[VP], t2[VP], tp[VP];
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+#pragma unroll
+      for (int v = 0; v < VP; v++) {
+        t1[v] = res[v].o1[f];
+        t2[v] = res[v].o2[f];
+      }
+      o1[f * vs + vo] = VT::pack(t1);
+      if (ST != 3) o2[f * vs + vo] = VT::pack(t2);
+    }
+    if (vp) {
+#pragma unroll
+      for (int v = 0; v < VP; v++) tp[v] = res[v].p;
+      vp[vo] = VT::pack(tp);
+    }
+  } else {  // the row's last valid column: store its point alone
+    const long long o = rb + q0;
+    cx<R> *s1 = ST == 3 ? sa.u0 : sa.next;
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      s1[f * g.slot + o] = res[0].o1[f];
+      if (ST != 3) sa.acc[f * g.slot + o] = res[0].o2[f];
+    }
+    if (sa.ph) sa.ph[o] = res[0].p;
   }
 }
 
