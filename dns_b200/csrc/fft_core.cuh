@@ -167,7 +167,7 @@ template <> struct Plan<32>  { static constexpr int E = 8,  NS = 2, R0 = 8,  R1 
 template <> struct Plan<64>  { static constexpr int E = 8,  NS = 2, R0 = 8,  R1 = 8, R2 = 1, R3 = 1; };
 template <> struct Plan<128> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 8, R2 = 1, R3 = 1; };
 template <> struct Plan<256> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 16, R2 = 1, R3 = 1; };
-template <> struct Plan<512> { static constexpr int E = 8,  NS = 3, R0 = 8,  R1 = 8, R2 = 8, R3 = 1; };
+template <> struct Plan<512> { static constexpr int E = 16, NS = 3, R0 = 16, R1 = 16, R2 = 2, R3 = 1; };
 
 // Plans for the full-length complex FFTs of the fused z pass: E = 8 values
 // per thread keeps the three u x omega accumulators in registers.

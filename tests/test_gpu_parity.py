@@ -184,6 +184,70 @@ def test_golden_0128_t1(dns, re_):
     assert de.max() <= E_TOL and do.max() <= E_TOL, (float(de.max()), float(do.max()))
 
 
+# ---------------------------------------------------------------- n = 512
+# No golden ships at 512^3 and the oracle would need ~30 GB of host memory
+# there, so the largest grid is checked through size-independent properties.
+
+
+def test_n512_tgv_spectrum_known_answer(dns):
+    """r2c of Taylor-Green at 512^3 against its exact spectrum: with FFTW's
+    unnormalised e^{-i} transform, U_hat = -i s_x n^3 / 8 and
+    V_hat = +i s_y n^3 / 8 at k = (s_x, s_y, 1), s = +-1, and zero elsewhere
+    on the half spectrum; E = 1/8 and Omega = 3/8 (main.c's scaling)."""
+    n = 512
+    U, V, W, _ = dns.tgv_fields(n)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(U, V, W)
+        del U, V, W
+        e, w = ctx.diagnostics()
+        uh = ctx.get_spectral()
+    a = n ** 3 / 8
+    for sx in (1, -1):
+        for sy in (1, -1):
+            i, j = sx % n, sy % n
+            uh[0, i, j, 1] -= -1j * sx * a
+            uh[1, i, j, 1] -= 1j * sy * a
+    err = float(np.abs(uh).max()) / a
+    assert err <= 1e-13, err
+    assert abs(float(e) - 0.125) <= 1e-14 and abs(float(w) - 0.375) <= 1e-14, (e, w)
+
+
+def test_n512_matches_n256_while_resolved(dns):
+    """20 steps of Taylor-Green (nu = 1/1600, dt = 0.0025) at 512^3 and at
+    256^3: at t = 0.05 the spectrum beyond |k| = 85 is far below rounding,
+    so both grids give the same energy and enstrophy to rounding."""
+    nu, dt = float("%.16e" % (1.0 / 1600)), 0.0025
+    out = {}
+    for n in (256, 512):
+        U, V, W, _ = dns.tgv_fields(n)
+        with dns.Context(n) as ctx:
+            ctx.set_velocity(U, V, W)
+            del U, V, W
+            hist = []
+            for q in range(3):
+                if q:
+                    ctx.step(nu, dt, 10)
+                hist.append(ctx.diagnostics())
+        out[n] = np.array(hist, dtype=np.longdouble)
+    rel = np.abs(out[512] - out[256]) / np.abs(out[256])
+    assert float(rel.max()) <= E_TOL, rel
+
+
+def test_n512_mixed_tracks_fp64(dns):
+    """The mixed path at 512^3 stays within FP32 rounding of the FP64 path
+    over 20 Taylor-Green steps."""
+    n, nu, dt = 512, float("%.16e" % (1.0 / 1600)), 0.0025
+    U, V, W, _ = dns.tgv_fields(n)
+    res = []
+    for prec in (dns.DNS_PREC_FP64, dns.DNS_PREC_MIXED):
+        with dns.Context(n, precision=prec) as ctx:
+            ctx.set_velocity(U, V, W)
+            ctx.step(nu, dt, 20)
+            res.append(np.array(ctx.diagnostics(), dtype=np.float64))
+    rel = np.abs(res[1] - res[0]) / np.abs(res[0])
+    assert float(rel.max()) <= 1e-5, rel
+
+
 @pytest.mark.parametrize("re_", ["0100", "1600", "3000"])
 def test_golden_0256_full(dns, re_):
     """256^3 Taylor-Green against the reference's FFTW history over the
