@@ -79,11 +79,13 @@ def test_adjoint_torch_autograd(dns):
     assert nut.grad.item() == 3.0 * gnu
 
 
-def test_adjoint_config_128(dns):
+@pytest.mark.parametrize("n", [128, 256])
+def test_adjoint_config(dns, n):
     """Config: random isotropic solenoidal field, E(k) ~ k^4 exp(-2 (k/4)^2),
-    unit energy (main.c's half-spectrum E), 128^3, nu = 0.005, dt = 0.005,
-    T = 2 (401 steps by main.c's loop), 20 snapshots, 8 seeded directions."""
-    n, nu, dt = 128, 0.005, 0.005
+    unit energy (main.c's half-spectrum E), 128^3 and 256^3, nu = 0.005,
+    dt = 0.005, T = 2 (401 steps by main.c's loop), 20 snapshots, 8 seeded
+    directions."""
+    nu, dt = 0.005, 0.005
     _, nsteps = dns.step_schedule(2.0, dt)
     assert nsteps == 401
     u0 = dns.solenoidal_perturbation(n, seed=0)
