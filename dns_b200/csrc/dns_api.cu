@@ -199,7 +199,8 @@ struct Ops {
   template <int AXIS>
   static constexpr size_t COL_SMEM = (size_t)(N + N * CW<AXIS>) * sizeof(C);
   static constexpr size_t Z_SMEM = (size_t)(2 * N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(C);
-  static constexpr size_t ZS_SMEM = ZC<R, N>::SMEM;
+  template <int KIND>
+  static constexpr size_t ZS_SMEM = ZC<R, N, KIND>::SMEM;
 
   template <class K>
   static cudaError_t allow(K kern, size_t smem) {
@@ -211,9 +212,9 @@ struct Ops {
     if ((e = allow(k_colpass<R, N, 0, true>, COL_SMEM<0>))) return e;
     if ((e = allow(k_colpass<R, N, 1, false>, COL_SMEM<1>))) return e;
     if ((e = allow(k_colpass<R, N, 1, true>, COL_SMEM<1>))) return e;
-    if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM))) return e;
-    if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM))) return e;
-    if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM))) return e;
+    if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM<0>))) return e;
+    if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM<1>))) return e;
+    if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM<2>))) return e;
     if ((e = allow(k_zr2c<R, N>, Z_SMEM))) return e;
     if ((e = allow(k_zc2r<R, N>, Z_SMEM))) return e;
     return cudaSuccess;
@@ -234,8 +235,9 @@ struct Ops {
   }
 
   static dim3 zgrid(int nfields) { return dim3((N * N) / ZCfg<N>::LINES, nfields); }
+  template <int KIND>
   static dim3 zsgrid(int nruns) {
-    return dim3((N * N + ZC<R, N>::LINES - 1) / ZC<R, N>::LINES, nruns);
+    return dim3((N * N + ZC<R, N, KIND>::LINES - 1) / ZC<R, N, KIND>::LINES, nruns);
   }
 
   // kernel `k` (0..KERNELS_PER_STAGE-1) of RK stage `s`, all runs of G
@@ -253,11 +255,11 @@ struct Ops {
         break;
       case 2:
         if (s == 0)
-          k_zstage<R, N, 0><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
+          k_zstage<R, N, 0><<<zsgrid<0>(G.nruns), ZC<R, N, 0>::THREADS, ZS_SMEM<0>, st>>>(work, stale, tw(G), g, invn3);
         else if (s < 3)
-          k_zstage<R, N, 1><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
+          k_zstage<R, N, 1><<<zsgrid<1>(G.nruns), ZC<R, N, 1>::THREADS, ZS_SMEM<1>, st>>>(work, stale, tw(G), g, invn3);
         else
-          k_zstage<R, N, 2><<<zsgrid(G.nruns), ZC<R, N>::THREADS, ZS_SMEM, st>>>(work, stale, tw(G), g, invn3);
+          k_zstage<R, N, 2><<<zsgrid<2>(G.nruns), ZC<R, N, 2>::THREADS, ZS_SMEM<2>, st>>>(work, stale, tw(G), g, invn3);
         break;
       case 3:
       case 4: {

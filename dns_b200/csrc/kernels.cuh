@@ -32,6 +32,8 @@
 #pragma once
 #include "fft_core.cuh"
 
+#include <type_traits>
+
 namespace dnsb {
 
 // work slots of the stage
@@ -325,28 +327,38 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
 // ---------------------------------------------------------------------------
-template <class R, int N>
+// FP64 first/last stage: 8 values per thread (the velocity and partial sums
+// are staged, N accumulates in registers).  FP64 middle stage and FP32: the
+// column plans, up to 16 values per thread and one exchange fewer per FFT
+// at n = 128, 256.
+template <class R, int N, int KIND>
 struct ZPlanFor {
-  using P = ZFPlan<N>;  // FP64: 8 values per thread (registers)
+  using P = typename std::conditional<KIND == 1, Plan<N>, ZFPlan<N>>::type;
 };
-template <int N>
-struct ZPlanFor<float, N> {
-  using P = Plan<N>;    // FP32: up to 16 values per thread, fewer exchanges
+template <int N, int KIND>
+struct ZPlanFor<float, N, KIND> {
+  using P = Plan<N>;
 };
 
-template <class R, int N>
+template <class R, int N, int KIND>
 struct ZC {
-  using P = typename ZPlanFor<R, N>::P;
+  using P = typename ZPlanFor<R, N, KIND>::P;
   static constexpr int E = P::E;
   static constexpr int T = N / E;                 // threads per line
   static constexpr int M = N / 2;
-  static constexpr int WANT = 128;
+  // FP64 middle stage with 16 values per thread: (u, omega_y), then
+  // (w, omega_z), wait in shared memory for the next pair's FFT while
+  // N_x, N_y, N_z stay in registers (up to 255 of them, 64-thread blocks)
+  static constexpr bool S2 = KIND == 1 && sizeof(R) == 8 && E >= 16;
+  static constexpr int WANT = S2 ? 64 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
-  static constexpr int MINB = 3;                  // blocks per SM (caps registers at 170)
+  static constexpr int MINB = S2 ? 4 : 3;         // blocks per SM (register cap 255 / 170)
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
-  static constexpr int STASH = 5 * N;             // scalars per line: u, v, w, N_y, N_z
+  // staged scalars per line: first/last stage u, v, w, N_y, N_z; middle
+  // stage two (S2) or none
+  static constexpr int STASH = KIND == 1 ? (S2 ? 2 * N : 0) : 5 * N;
   static constexpr size_t SMEM =
       (size_t)(N + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
 };
@@ -355,9 +367,9 @@ struct ZC {
 // Loads are issued in chunks of CH positions (an empty asm with a memory
 // clobber keeps the compiler from hoisting all of them), which bounds the
 // registers held by loads in flight.
-template <class R, int N, int CH = 4, class C, class FA, class FB>
-__device__ __forceinline__ void ext_pair(C (&y)[ZC<R, N>::E], int t, FA fa, FB fb) {
-  using Z = ZC<R, N>;
+template <class R, int N, int KIND, int CH = 4, class C, class FA, class FB>
+__device__ __forceinline__ void ext_pair(C (&y)[ZC<R, N, KIND>::E], int t, FA fa, FB fb) {
+  using Z = ZC<R, N, KIND>;
 #pragma unroll
   for (int e0 = 0; e0 < Z::E; e0 += CH) {
 #pragma unroll
@@ -382,9 +394,9 @@ __device__ __forceinline__ void ext_pair(C (&y)[ZC<R, N>::E], int t, FA fa, FB f
 
 // Same, with one functor giving both spectra at a position, so that a field
 // feeding both halves (u for u and omega_y) is loaded once.
-template <class R, int N, int CH = 4, class C, class FAB>
-__device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N>::E], int t, FAB fab) {
-  using Z = ZC<R, N>;
+template <class R, int N, int KIND, int CH = 4, class C, class FAB>
+__device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N, KIND>::E], int t, FAB fab) {
+  using Z = ZC<R, N, KIND>;
 #pragma unroll
   for (int e0 = 0; e0 < Z::E; e0 += CH) {
 #pragma unroll
@@ -409,11 +421,11 @@ __device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N>::E], int t, FAB fab) {
 }
 
 template <class R, int N, int KIND>
-__global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
+__global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     k_zstage(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg, Geo g,
              R invn3) {
   using C = cx<R>;
-  using Z = ZC<R, N>;
+  using Z = ZC<R, N, KIND>;
   constexpr int E = Z::E, T = Z::T, M = Z::M;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = (C *)smem_raw;  // stage twiddles of the z plan (<= N entries)
@@ -460,7 +472,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
 #pragma unroll
       for (int f = 0; f < 3; f++) SU_(f, e) = ok ? stale[f * g.nreal + roff + m] : R(0);
     }
-    ext_pair<R, N>(y, t, f_ox, f_oy);
+    ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -470,13 +482,56 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       ny[e] = w * ox;
       nz[e] = u * oy - v * ox;
     }
-    ext_pair<R, N>(y, t, f_oz, f_zero);
+    ext_pair<R, N, KIND>(y, t, f_oz, f_zero);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const R oz = y[e].x * invn3;
       nx[e] += SU_(1, e) * oz;
       ny[e] -= SU_(0, e) * oz;
+    }
+  } else if (KIND == 1 && Z::S2) {
+    // the same pairs as below; u, omega_y and then w, omega_z are staged
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+      const C uu = ld(pU, s), d = ld(pDWDX, s);
+      a = uu;
+      b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R u = y[e].x * invn3, oy = y[e].y * invn3;
+      nz[e] = u * oy;
+      SU_(0, e) = u;
+      SU_(1, e) = oy;
+    }
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+      a = ld(pW, s);
+      b = csub(ld(pDVDX, s), ld(pDUDY, s));  // dv/dx - du/dy
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R w = y[e].x * invn3, oz = y[e].y * invn3;
+      const R u = SU_(0, e), oy = SU_(1, e);
+      nx[e] = -w * oy;
+      ny[e] = -u * oz;
+      SU_(0, e) = w;
+      SU_(1, e) = oz;
+    }
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+      const C vv = ld(pV, s), d = ld(pDWDY, s);
+      a = vv;
+      b = cmk<C>(d.x + (R)s * vv.y, d.y - (R)s * vv.x);  // dw/dy - i kz v
+    });
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R v = y[e].x * invn3, ox = y[e].y * invn3;
+      const R w = SU_(0, e), oz = SU_(1, e);
+      nx[e] += v * oz;
+      ny[e] += w * ox;
+      nz[e] -= v * ox;
     }
   } else if (KIND == 1) {
     // Pairs ordered so that every input slot is read once and the cross
@@ -485,7 +540,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
     //   (w, omega_z): N_x = -w oy, N_y = -u oz
     //   (v, omega_x): N_x += v oz, N_y += w ox, N_z -= v ox
     R u[E], oy[E];
-    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       const C uu = ld(pU, s), d = ld(pDWDX, s);
       a = uu;
       b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
@@ -497,7 +552,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       oy[e] = y[e].y * invn3;
       nz[e] = u[e] * oy[e];
     }
-    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       a = ld(pW, s);
       b = csub(ld(pDVDX, s), ld(pDUDY, s));  // dv/dx - du/dy
     });
@@ -510,7 +565,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       nx[e] = -w[e] * oy[e];
       ny[e] = -u[e] * oz[e];
     }
-    ext_gen<R, N>(y, t, [&](int s, C &a, C &b) {
+    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       const C vv = ld(pV, s), d = ld(pDWDY, s);
       a = vv;
       b = cmk<C>(d.x + (R)s * vv.y, d.y - (R)s * vv.x);  // dw/dy - i kz v
@@ -527,7 +582,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
     // last stage: the velocity is also stored as the next stale one, so it
     // is staged in shared memory (the register-only order above spills here)
     // (u, v)
-    ext_pair<R, N>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
+    ext_pair<R, N, KIND>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -535,7 +590,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       SU_(1, e) = y[e].y * invn3;
     }
     // (w, omega_x)
-    ext_pair<R, N>(y, t, [&](int s) { return ld(pW, s); }, f_ox);
+    ext_pair<R, N, KIND>(y, t, [&](int s) { return ld(pW, s); }, f_ox);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -545,7 +600,7 @@ __global__ void __launch_bounds__(ZC<R, N>::THREADS, ZC<R, N>::MINB)
       SU_(4, e) = -SU_(1, e) * ox;   // partial N_z
     }
     // (omega_y, omega_z)
-    ext_pair<R, N>(y, t, f_oy, f_oz);
+    ext_pair<R, N, KIND>(y, t, f_oy, f_oz);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
