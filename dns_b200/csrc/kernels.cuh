@@ -32,8 +32,6 @@
 #pragma once
 #include "fft_core.cuh"
 
-#include <type_traits>
-
 namespace dnsb {
 
 // work slots of the stage
@@ -327,13 +325,11 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
 // ---------------------------------------------------------------------------
-// FP64 first/last stage: 8 values per thread (the velocity and partial sums
-// are staged, N accumulates in registers).  FP64 middle stage and FP32: the
-// column plans, up to 16 values per thread and one exchange fewer per FFT
-// at n = 128, 256.
+// The column plans: up to 16 values per thread, one exchange fewer per FFT
+// than 8 values at n = 128, 256.
 template <class R, int N, int KIND>
 struct ZPlanFor {
-  using P = typename std::conditional<KIND == 1, Plan<N>, ZFPlan<N>>::type;
+  using P = Plan<N>;
 };
 template <int N, int KIND>
 struct ZPlanFor<float, N, KIND> {
@@ -346,19 +342,22 @@ struct ZC {
   static constexpr int E = P::E;
   static constexpr int T = N / E;                 // threads per line
   static constexpr int M = N / 2;
-  // FP64 middle stage with 16 values per thread: (u, omega_y), then
-  // (w, omega_z), wait in shared memory for the next pair's FFT while
-  // N_x, N_y, N_z stay in registers (up to 255 of them, 64-thread blocks)
-  static constexpr bool S2 = KIND == 1 && sizeof(R) == 8 && E >= 16;
+  // FP64 with 16 values per thread: N_x, N_y, N_z stay in registers (up to
+  // 255 of them, 64-thread blocks); in the middle and last stages (u,
+  // omega_y), then (w, omega_z), wait in shared memory for the next pair's
+  // FFT, and the first stage reads the stale velocity where it needs it
+  static constexpr bool S2 = sizeof(R) == 8 && E >= 16;
   static constexpr int WANT = S2 ? 64 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
   static constexpr int MINB = S2 ? 4 : 3;         // blocks per SM (register cap 255 / 170)
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
-  // staged scalars per line: first/last stage u, v, w, N_y, N_z; middle
-  // stage two (S2) or none
-  static constexpr int STASH = KIND == 1 ? (S2 ? 2 * N : 0) : 5 * N;
+  // staged scalars per line: S2 none (first stage), two (middle stage) or
+  // three (last stage, u kept for the stale store); FP32 none (middle
+  // stage) or u, v, w, N_y, N_z (first and last stage)
+  static constexpr int STASH =
+      S2 ? (KIND == 0 ? 0 : (KIND + 1) * N) : (KIND == 1 ? 0 : 5 * N);
   static constexpr size_t SMEM =
       (size_t)(N + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
 };
@@ -464,7 +463,28 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
 
   C y[E];
   R nx[E], ny[E], nz[E];
-  if (KIND == 0) {
+  if (KIND == 0 && Z::S2) {
+    // stale real velocity read where it is needed (L1/L2 hits the second time)
+    auto sv = [&](int f, int e) -> R { return ok ? stale[f * g.nreal + roff + t + T * e] : R(0); };
+    ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R ox = y[e].x * invn3, oy = y[e].y * invn3;
+      const R u = sv(0, e), v = sv(1, e), w = sv(2, e);
+      nx[e] = -w * oy;
+      ny[e] = w * ox;
+      nz[e] = u * oy - v * ox;
+    }
+    ext_pair<R, N, KIND>(y, t, f_oz, f_zero);
+    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const R oz = y[e].x * invn3;
+      nx[e] += sv(1, e) * oz;
+      ny[e] -= sv(0, e) * oz;
+    }
+  } else if (KIND == 0) {
     // stale real velocity, own points m = t + T e
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -490,8 +510,9 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       nx[e] += SU_(1, e) * oz;
       ny[e] -= SU_(0, e) * oz;
     }
-  } else if (KIND == 1 && Z::S2) {
-    // the same pairs as below; u, omega_y and then w, omega_z are staged
+  } else if (Z::S2) {
+    // the middle stage's pairs; u, omega_y and then w, omega_z are staged;
+    // the last stage also stores the velocity as the next stale one
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       const C uu = ld(pU, s), d = ld(pDWDX, s);
       a = uu;
@@ -504,6 +525,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       nz[e] = u * oy;
       SU_(0, e) = u;
       SU_(1, e) = oy;
+      if (KIND == 2) SU_(2, e) = u;
     }
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       a = ld(pW, s);
@@ -532,6 +554,17 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       nx[e] += v * oz;
       ny[e] += w * ox;
       nz[e] -= v * ox;
+      if (KIND == 2) SU_(1, e) = v;
+    }
+    if (KIND == 2 && ok) {
+      // the velocity becomes the next step's stale one (u, v, w staged)
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const long long m = roff + t + T * e;
+        stale[m] = SU_(2, e);
+        stale[g.nreal + m] = SU_(1, e);
+        stale[2 * g.nreal + m] = SU_(0, e);
+      }
     }
   } else if (KIND == 1) {
     // Pairs ordered so that every input slot is read once and the cross
