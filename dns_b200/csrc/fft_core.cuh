@@ -169,18 +169,6 @@ template <> struct Plan<128> { static constexpr int E = 16, NS = 2, R0 = 16, R1 
 template <> struct Plan<256> { static constexpr int E = 16, NS = 2, R0 = 16, R1 = 16, R2 = 1, R3 = 1; };
 template <> struct Plan<512> { static constexpr int E = 16, NS = 3, R0 = 16, R1 = 16, R2 = 2, R3 = 1; };
 
-// Plans for the full-length complex FFTs of the fused z pass: E = 8 values
-// per thread keeps the three u x omega accumulators in registers.
-template <int L>
-struct ZFPlan;
-template <> struct ZFPlan<8>   { static constexpr int E = 8, NS = 1, R0 = 8, R1 = 1, R2 = 1, R3 = 1; };
-template <> struct ZFPlan<16>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 2, R2 = 1, R3 = 1; };
-template <> struct ZFPlan<32>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 4, R2 = 1, R3 = 1; };
-template <> struct ZFPlan<64>  { static constexpr int E = 8, NS = 2, R0 = 8, R1 = 8, R2 = 1, R3 = 1; };
-template <> struct ZFPlan<128> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 2, R3 = 1; };
-template <> struct ZFPlan<256> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 4, R3 = 1; };
-template <> struct ZFPlan<512> { static constexpr int E = 8, NS = 3, R0 = 8, R1 = 8, R2 = 8, R3 = 1; };
-
 // Plans for the half-length complex FFT of the z (real) axis, one warp or
 // less per line: E <= 8 keeps registers free for the fused pointwise work.
 template <int M>

@@ -325,20 +325,11 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
 //         the back transform at rk == 0); KIND 1: middle stage;
 // KIND 2: last stage, also stores the real velocity as the next stale one.
 // ---------------------------------------------------------------------------
-// The column plans: up to 16 values per thread, one exchange fewer per FFT
-// than 8 values at n = 128, 256.
-template <class R, int N, int KIND>
-struct ZPlanFor {
-  using P = Plan<N>;
-};
-template <int N, int KIND>
-struct ZPlanFor<float, N, KIND> {
-  using P = Plan<N>;
-};
-
+// The z pass runs the column plans: up to 16 values per thread, one exchange
+// fewer per FFT than 8 values at n = 128, 256.
 template <class R, int N, int KIND>
 struct ZC {
-  using P = typename ZPlanFor<R, N, KIND>::P;
+  using P = Plan<N>;
   static constexpr int E = P::E;
   static constexpr int T = N / E;                 // threads per line
   static constexpr int M = N / 2;
