@@ -49,13 +49,16 @@ def pass_units(pressure: bool = False):
     u = []
     for s in range(4):
         a = (3 + 5, 0)
-        b = (5 + 6, 0) if s == 0 else (5 + 7, 0)
+        # B reads u, dv/dx, v, w, dw/dx; writes u, omega_z, v, (w), dw/dy, dw/dx
+        b = (5 + 5, 0) if s == 0 else (5 + 6, 0)
+        # C reads u, v, (w), dw/dx, dw/dy, omega_z (+ the stale velocity in
+        # stage 0, + its store in stage 3) and writes N
         if s == 0:
-            c = (6 + 3, 3)
+            c = (5 + 3, 3)
         elif s < 3:
-            c = (7 + 3, 0)
+            c = (6 + 3, 0)
         else:
-            c = (7 + 3, 3)
+            c = (6 + 3, 3)
         d = (3 + 3, 0)
         e1 = (3 + 3, 0)
         if s == 0:

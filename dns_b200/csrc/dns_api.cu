@@ -158,7 +158,8 @@ constexpr double RK_B[3] = {0.5, 0.5, 1.0};                       // main.c:16
 
 ColJobs jobs_empty(int njobs) {
   ColJobs j;
-  for (int q = 0; q < 8; q++) j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1;
+  for (int q = 0; q < 8; q++)
+    j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1, j.add_slot[q] = -1;
   j.njobs = njobs;
   return j;
 }
@@ -166,19 +167,19 @@ ColJobs jobs_pass_a(int in0) {
   ColJobs j = jobs_empty(3);
   const int w = SLOT_WORK;
   j.in_slot[0] = in0 + 0; j.out_slot[0] = w + SU;
-  j.in_slot[1] = in0 + 1; j.out_slot[1] = w + SV; j.der_slot[1] = w + SDVDX;
+  j.in_slot[1] = in0 + 1; j.out_slot[1] = w + SV; j.der_slot[1] = w + SOMZ;  // dv/dx
   j.in_slot[2] = in0 + 2; j.out_slot[2] = w + SW; j.der_slot[2] = w + SDWDX;
   return j;
 }
 ColJobs jobs_pass_b(bool first) {
-  ColJobs j = jobs_empty(5);
+  ColJobs j = jobs_empty(4);
   const int w = SLOT_WORK;
-  j.in_slot[0] = w + SU; j.out_slot[0] = w + SU; j.der_slot[0] = w + SDUDY;
+  // u, and omega_z = dv/dx - i ky u over the dv/dx slot (same tile, same block)
+  j.in_slot[0] = w + SU; j.out_slot[0] = w + SU; j.der_slot[0] = w + SOMZ; j.add_slot[0] = w + SOMZ;
   j.in_slot[1] = w + SV; j.out_slot[1] = w + SV;
   // the first stage reads the stale real velocity, so W itself is not needed
   j.in_slot[2] = w + SW; j.out_slot[2] = first ? -1 : w + SW; j.der_slot[2] = w + SDWDY;
-  j.in_slot[3] = w + SDVDX; j.out_slot[3] = w + SDVDX;
-  j.in_slot[4] = w + SDWDX; j.out_slot[4] = w + SDWDX;
+  j.in_slot[3] = w + SDWDX; j.out_slot[3] = w + SDWDX;
   return j;
 }
 ColJobs jobs_map(const int *in, const int *out, int cnt) {

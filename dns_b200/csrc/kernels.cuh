@@ -19,8 +19,8 @@
 //
 // One RK stage = six kernels:
 //   A   x backward  state (3) -> u,v,w and d/dx of v,w            (per field)
-//   B   y backward  5 slots -> u,v,w, dv/dx, dw/dx, du/dy, dw/dy    (per field)
-//   C   z pass      per z line: vorticity from the 7 slots, u and omega to
+//   B   y backward  5 slots -> u,v,w, omega_z = dv/dx - du/dy, dw/dx, dw/dy
+//   C   z pass      per z line: vorticity from the 6 slots, u and omega to
 //                   real space, N = u x omega, N back to z spectral; real
 //                   space touches HBM only for the stale velocity
 //   D   y forward   3 slots, in place
@@ -34,8 +34,9 @@
 
 namespace dnsb {
 
-// work slots of the stage
-enum { SU = 0, SV = 1, SW = 2, SDVDX = 3, SDWDX = 4, SDUDY = 5, SDWDY = 6, NWORK = 7 };
+// work slots of the stage (after pass B, SOMZ holds omega_z = dv/dx - du/dy;
+// after pass A it holds dv/dx)
+enum { SU = 0, SV = 1, SW = 2, SOMZ = 3, SDWDX = 4, SDWDY = 5, NWORK = 6 };
 
 struct Geo {
   int n, nf, nfp;
@@ -49,11 +50,13 @@ struct Geo {
 // A column pass processes tiles of W adjacent kz columns x the full line
 // along x or y.  block.z = job + njobs * run: each job maps an input slot to
 // an output slot and optionally the derivative i*k*f (k along the pass axis)
-// to a der slot, in every run of the batch.
+// to a der slot, in every run of the batch; with an add slot the derivative
+// output is add - i*k*f instead (the same tile of another slot).
 struct ColJobs {
   int in_slot[8];
   int out_slot[8];   // -1: no plain output
   int der_slot[8];   // -1: no derivative output
+  int add_slot[8];   // -1: none
   int njobs;
 };
 
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
     rs = g.nfp;
   }
   const C *src = in + (long long)jobs.in_slot[job] * g.slot + base;
-  const int oslot = jobs.out_slot[job], dslot = jobs.der_slot[job];
+  const int oslot = jobs.out_slot[job], dslot = jobs.der_slot[job], aslot = jobs.add_slot[job];
   C v[E];
   // the input is read twice (the second read is an L2 hit) rather than kept
   // in a second register array: first for the derivative i k f, then for the
@@ -140,11 +143,19 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
     if (dst_slot < 0) continue;
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = ok ? src[(t + T * e) * rs] : czero<C>();
-    if (pass == 0) {
+    if (pass == 0 && aslot < 0) {
 #pragma unroll
       for (int e = 0; e < E; e++) {
         const R k = (R)kwave(t + T * e, N);
         v[e] = cmk<C>(-k * v[e].y, k * v[e].x);  // i k f
+      }
+    } else if (pass == 0) {
+      const C *add = in + (long long)aslot * g.slot + base;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const R k = (R)kwave(t + T * e, N);
+        const C a = ok ? add[(t + T * e) * rs] : czero<C>();
+        v[e] = cmk<C>(a.x + k * v[e].y, a.y - k * v[e].x);  // add - i k f
       }
     }
     line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, BlockSync{});
@@ -432,8 +443,8 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
   stale += (long long)blockIdx.y * g.run_real;
   const long long off = line * g.nfp;
   const C *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
-  const C *pW = work + SW * g.slot + off, *pDVDX = work + SDVDX * g.slot + off;
-  const C *pDWDX = work + SDWDX * g.slot + off, *pDUDY = work + SDUDY * g.slot + off;
+  const C *pW = work + SW * g.slot + off, *pOMZ = work + SOMZ * g.slot + off;
+  const C *pDWDX = work + SDWDX * g.slot + off;
   const C *pDWDY = work + SDWDY * g.slot + off;
   auto ld = [&](const C *p, int s) -> C { return ok ? p[s] : czero<C>(); };
   auto f_ox = [&](int s) -> C {  // omega_x = dw/dy - i kz v
@@ -445,7 +456,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     return cmk<C>(-(R)s * u.y - b.x, (R)s * u.x - b.y);
   };
   auto f_oz = [&](int s) -> C {  // omega_z = dv/dx - du/dy
-    return csub(ld(pDVDX, s), ld(pDUDY, s));
+    return ld(pOMZ, s);
   };
   auto f_zero = [&](int) -> C { return czero<C>(); };
   const LineSync<(T > 32)> sync{};
@@ -520,7 +531,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     }
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       a = ld(pW, s);
-      b = csub(ld(pDVDX, s), ld(pDUDY, s));  // dv/dx - du/dy
+      b = ld(pOMZ, s);
     });
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
@@ -578,7 +589,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     }
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       a = ld(pW, s);
-      b = csub(ld(pDVDX, s), ld(pDUDY, s));  // dv/dx - du/dy
+      b = ld(pOMZ, s);
     });
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
     R w[E], oz[E];
