@@ -203,16 +203,26 @@ struct Ops {
   template <int KIND>
   static constexpr size_t ZS_SMEM = ZC<R, N, KIND>::SMEM;
 
+  // the column-pass kernel of this precision and size: FP32 n = 256 tiles run
+  // the variant held to 4 blocks per SM
+  template <int AXIS, bool FWD>
+  static auto colkern() {
+    if constexpr (sizeof(R) == 4 && N == 256)
+      return k_colpass_minb<R, N, AXIS, FWD, 4>;
+    else
+      return k_colpass<R, N, AXIS, FWD>;
+  }
+
   template <class K>
   static cudaError_t allow(K kern, size_t smem) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
   static cudaError_t setup() {
     cudaError_t e;
-    if ((e = allow(k_colpass<R, N, 0, false>, COL_SMEM<0>))) return e;
-    if ((e = allow(k_colpass<R, N, 0, true>, COL_SMEM<0>))) return e;
-    if ((e = allow(k_colpass<R, N, 1, false>, COL_SMEM<1>))) return e;
-    if ((e = allow(k_colpass<R, N, 1, true>, COL_SMEM<1>))) return e;
+    if ((e = allow(colkern<0, false>(), COL_SMEM<0>))) return e;
+    if ((e = allow(colkern<0, true>(), COL_SMEM<0>))) return e;
+    if ((e = allow(colkern<1, false>(), COL_SMEM<1>))) return e;
+    if ((e = allow(colkern<1, true>(), COL_SMEM<1>))) return e;
     if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM<0>))) return e;
     if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM<1>))) return e;
     if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM<2>))) return e;
@@ -228,7 +238,7 @@ struct Ops {
   static void colpass_io(const Group &G, cudaStream_t st, const C *in, C *out, const ColJobs &jobs,
                          int nruns) {
     dim3 grid(G.g.nfp / CW<AXIS>, N, jobs.njobs * nruns);
-    k_colpass<R, N, AXIS, FWD><<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
+    colkern<AXIS, FWD>()<<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
   }
   template <int AXIS, bool FWD>
   static void colpass(const Group &G, cudaStream_t st, const ColJobs &jobs) {

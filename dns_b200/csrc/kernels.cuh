@@ -104,9 +104,9 @@ struct LineSync {
 // (W = ColW<R, AXIS, N>::W).
 // ---------------------------------------------------------------------------
 template <class R, int N, int AXIS, bool FWD>
-__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
-    k_colpass(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
-              const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
+__device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
+                                             const cx<R> *__restrict__ twg, const Geo &g,
+                                             const ColJobs &jobs) {
   using C = cx<R>;
   constexpr int W = ColW<R, AXIS, N>::W;
   constexpr int E = Plan<N>::E, T = N / E;
@@ -165,6 +165,25 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
       for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = v[e];
     }
   }
+}
+
+template <class R, int N, int AXIS, bool FWD>
+__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
+    k_colpass(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
+              const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
+  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs);
+}
+
+// The same pass with its registers held so that MINB blocks fit per SM: the
+// FP32 tiles at n = 256 (256 threads) run 4 blocks at <= 64 registers (the
+// omega_z job's second tile would otherwise take 66, 3 blocks).  An explicit
+// ceiling is not applied to the other tiles: with one, the compiler trades
+// their occupancy for registers.
+template <class R, int N, int AXIS, bool FWD, int MINB>
+__global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W, MINB)
+    k_colpass_minb(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
+                   const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
+  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs);
 }
 
 // ---------------------------------------------------------------------------
