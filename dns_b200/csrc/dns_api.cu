@@ -7,7 +7,8 @@
 //     0..2   SA   state at the start of a step (U_hat, V_hat, W_hat)
 //     3..5   SB   RK stage input (main.c's U_hat during stages 1-3)
 //     6..8   ACC  RK accumulator (main.c's U_hat1)
-//     9..15  WORK seven partially transformed fields of the stage
+//     9..15  WORK partially transformed fields of a stage (six used; all seven
+//            are the float64 staging area of the FP32 path's host transfers)
 //     16     P    pressure of the last stage
 //   stale real velocity [3][n^3] (main.c's U, V, W between steps)
 //   twiddles, reduction partials.
