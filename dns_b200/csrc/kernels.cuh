@@ -368,6 +368,8 @@ struct ZC {
   // omega_y), then (w, omega_z), wait in shared memory for the next pair's
   // FFT, and the first stage reads the stale velocity where it needs it
   static constexpr bool S2 = sizeof(R) == 8 && E >= 16;
+  // FP32: N in registers in every stage (half the registers of FP64)
+  static constexpr bool F32 = sizeof(R) == 4;
   static constexpr int WANT = S2 ? 64 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
@@ -375,10 +377,10 @@ struct ZC {
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
   // staged scalars per line: S2 none (first stage), two (middle stage) or
-  // three (last stage, u kept for the stale store); FP32 none (middle
-  // stage) or u, v, w, N_y, N_z (first and last stage)
+  // three (last stage, u kept for the stale store); FP32 none; FP64 with 8
+  // values per thread none (middle stage) or u, v, w, N_y, N_z
   static constexpr int STASH =
-      S2 ? (KIND == 0 ? 0 : (KIND + 1) * N) : (KIND == 1 ? 0 : 5 * N);
+      S2 ? (KIND == 0 ? 0 : (KIND + 1) * N) : ((KIND == 1 || F32) ? 0 : 5 * N);
   static constexpr size_t SMEM =
       (size_t)(N + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
 };
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
 
   C y[E];
   R nx[E], ny[E], nz[E];
-  if (KIND == 0 && Z::S2) {
+  if (KIND == 0 && (Z::S2 || Z::F32)) {
     // stale real velocity read where it is needed (L1/L2 hits the second time)
     auto sv = [&](int f, int e) -> R { return ok ? stale[f * g.nreal + roff + t + T * e] : R(0); };
     ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
@@ -587,9 +589,10 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
         stale[2 * g.nreal + m] = SU_(0, e);
       }
     }
-  } else if (KIND == 1) {
+  } else if (KIND == 1 || Z::F32) {
     // Pairs ordered so that every input slot is read once and the cross
-    // product accumulates in registers:
+    // product accumulates in registers (FP32 last stage: the velocity is
+    // stored as the next stale one as it comes):
     //   (u, omega_y): N_z = u oy
     //   (w, omega_z): N_x = -w oy, N_y = -u oz
     //   (v, omega_x): N_x += v oz, N_y += w ox, N_z -= v ox
@@ -605,6 +608,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       u[e] = y[e].x * invn3;
       oy[e] = y[e].y * invn3;
       nz[e] = u[e] * oy[e];
+      if (KIND == 2 && ok) stale[roff + t + T * e] = u[e];
     }
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       a = ld(pW, s);
@@ -618,6 +622,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       oz[e] = y[e].y * invn3;
       nx[e] = -w[e] * oy[e];
       ny[e] = -u[e] * oz[e];
+      if (KIND == 2 && ok) stale[2 * g.nreal + roff + t + T * e] = w[e];
     }
     ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
       const C vv = ld(pV, s), d = ld(pDWDY, s);
@@ -631,10 +636,12 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       nx[e] += v * oz[e];
       ny[e] += w[e] * ox;
       nz[e] -= v * ox;
+      if (KIND == 2 && ok) stale[g.nreal + roff + t + T * e] = v;
     }
   } else {
-    // last stage: the velocity is also stored as the next stale one, so it
-    // is staged in shared memory (the register-only order above spills here)
+    // FP64 last stage at 8 values per thread: the velocity is also stored as
+    // the next stale one, so it is staged in shared memory (the register-only
+    // order above spills here)
     // (u, v)
     ext_pair<R, N, KIND>(y, t, [&](int s) { return ld(pU, s); }, [&](int s) { return ld(pV, s); });
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
