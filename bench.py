@@ -42,31 +42,47 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
 
 
+def mask_fractions(n: int):
+    """Fractions of the half spectrum's kz columns and of the kx (or ky)
+    indices inside the 2/3 rule of main.c:231-238 (|k| < 2/3 (n/2 + 1))."""
+    kmax = 2.0 / 3.0 * (n // 2 + 1)
+    kcut = -1
+    while kcut + 1 < kmax:
+        kcut += 1
+    fz = min(kcut + 1, n // 2 + 1) / (n // 2 + 1)
+    fxy = min(2 * kcut + 1, n) / n
+    return fz, fxy
+
+
 # algorithmic HBM traffic per launch of each pass, in units of one complex
 # half-spectrum field (n*n*(n/2+1)*16 bytes) and one real field (n^3 * 8)
-# [stage][pass] -> (complex fields moved, real fields moved)
-def pass_units(pressure: bool = False):
+# [stage][pass] -> (complex fields moved, real fields moved).  N is needed
+# only inside the 2/3 rule: C stores kz <= kcut, D and E1 move the masked
+# part, E2 reads N there only.
+def pass_units(n: int, pressure: bool = False):
+    fz, fxy = mask_fractions(n)
     u = []
     for s in range(4):
         a = (3 + 5, 0)
         # B reads u, dv/dx, v, w, dw/dx; writes u, omega_z, v, (w), dw/dy, dw/dx
         b = (5 + 5, 0) if s == 0 else (5 + 6, 0)
         # C reads u, v, (w), dw/dx, dw/dy, omega_z (+ the stale velocity in
-        # stage 0, + its store in stage 3) and writes N
+        # stage 0, + its store in stage 3) and writes N for kz <= kcut
         if s == 0:
-            c = (5 + 3, 3)
+            c = (5 + 3 * fz, 3)
         elif s < 3:
-            c = (6 + 3, 0)
+            c = (6 + 3 * fz, 0)
         else:
-            c = (6 + 3, 3)
-        d = (3 + 3, 0)
-        e1 = (3 + 3, 0)
+            c = (6 + 3 * fz, 3)
+        d = (3 * fz + 3 * fz * fxy, 0)
+        e1 = (3 * fz * fxy + 3 * fz * fxy * fxy, 0)
+        nn = 3 * fz * fxy * fxy
         if s == 0:
-            e2 = (3 + 3 + 6, 0)
+            e2 = (nn + 3 + 6, 0)
         elif s < 3:
-            e2 = (3 + 9 + 6, 0)
+            e2 = (nn + 9 + 6, 0)
         else:
-            e2 = (3 + 6 + 3 + (1 if pressure else 0), 0)
+            e2 = (nn + 6 + 3 + (1 if pressure else 0), 0)
         u.append([a, b, c, d, e1, e2])
     return u
 
@@ -74,7 +90,7 @@ def pass_units(pressure: bool = False):
 def pass_bytes(n: int):
     cf = n * n * (n // 2 + 1) * 16
     rf = n ** 3 * 8
-    return [[uc * cf + ur * rf for (uc, ur) in st] for st in pass_units()]
+    return [[uc * cf + ur * rf for (uc, ur) in st] for st in pass_units(n)]
 
 
 def step_bytes_model(n: int) -> int:

@@ -162,6 +162,7 @@ ColJobs jobs_empty(int njobs) {
   for (int q = 0; q < 8; q++)
     j.in_slot[q] = 0, j.out_slot[q] = -1, j.der_slot[q] = -1, j.add_slot[q] = -1;
   j.njobs = njobs;
+  j.masked = 0;
   return j;
 }
 ColJobs jobs_pass_a(int in0) {
@@ -275,12 +276,15 @@ struct Ops {
         break;
       case 3:
       case 4: {
-        // D: y forward, E1: x forward (in place on the three N slots)
+        // D: y forward, E1: x forward (in place on the three N slots); only
+        // the modes inside the 2/3 rule are computed and stored
         const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+        ColJobs j = jobs_map(io, io, 3);
+        j.masked = 1;
         if (k == 3)
-          colpass<1, true>(G, st, jobs_map(io, io, 3));
+          colpass<1, true>(G, st, j);
         else
-          colpass<0, true>(G, st, jobs_map(io, io, 3));
+          colpass<0, true>(G, st, j);
         break;
       }
       default: {

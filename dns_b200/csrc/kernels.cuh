@@ -51,13 +51,18 @@ struct Geo {
 // along x or y.  block.z = job + njobs * run: each job maps an input slot to
 // an output slot and optionally the derivative i*k*f (k along the pass axis)
 // to a der slot, in every run of the batch; with an add slot the derivative
-// output is add - i*k*f instead (the same tile of another slot).
+// output is add - i*k*f instead (the same tile of another slot).  A masked
+// pass (the forward passes of N, whose result only enters the update inside
+// the 2/3 rule, main.c:381-386) skips tiles whose kz columns all exceed kcut,
+// in the x pass also ky rows beyond kcut, and stores only |k| <= kcut along
+// its own axis.
 struct ColJobs {
   int in_slot[8];
   int out_slot[8];   // -1: no plain output
   int der_slot[8];   // -1: no derivative output
   int add_slot[8];   // -1: none
   int njobs;
+  int masked;
 };
 
 // column tile width: 128-byte tile rows (wider rows for the x passes, whose
@@ -113,6 +118,13 @@ __device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R>
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *st = (C *)smem_raw;  // stage twiddles (<= N entries)
   C *xb = st + N;
+  if (jobs.masked) {  // whole block, before any barrier
+    if ((int)blockIdx.x * W > g.kcut) return;
+    if (AXIS == 0) {
+      const int ky = kwave(blockIdx.y, N);
+      if ((ky < 0 ? -ky : ky) > g.kcut) return;
+    }
+  }
   build_stage_tw<N, Plan<N>>(st, twg, N);
   __syncthreads();
   const int p = threadIdx.x % W, t = threadIdx.x / W;
@@ -162,7 +174,10 @@ __device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R>
     if (ok) {
       C *dst = out + (long long)dst_slot * g.slot + base;
 #pragma unroll
-      for (int e = 0; e < E; e++) dst[(t + T * e) * rs] = v[e];
+      for (int e = 0; e < E; e++) {
+        const int k = kwave(t + T * e, N);
+        if (!jobs.masked || (k < 0 ? -k : k) <= g.kcut) dst[(t + T * e) * rs] = v[e];
+      }
     }
   }
 }
@@ -680,7 +695,9 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       }
     }
   }
-  // forward: (N_x, N_y) as one complex FFT, then N_z  (main.c:378-380)
+  // forward: (N_x, N_y) as one complex FFT, then N_z  (main.c:378-380);
+  // only kz <= kcut is stored: N enters the update through the 2/3 rule only
+  const int KZ = g.kcut < M ? g.kcut : M;
 #pragma unroll
   for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
   line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
@@ -691,7 +708,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
-    if (k <= M) {
+    if (k <= KZ) {
       const C z = y[e], p = xb[idx((N - k) & (N - 1))];
       const C a = cmk<C>(R(0.5) * (z.x + p.x), R(0.5) * (z.y - p.y));  // (Z + conj P) / 2
       const C d = cmk<C>(R(0.5) * (z.x - p.x), R(0.5) * (z.y + p.y));  // (Z - conj P) / 2
@@ -709,7 +726,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
-    if (k <= M && ok) oW[k] = y[e];
+    if (k <= KZ && ok) oW[k] = y[e];
   }
 }
 
@@ -765,10 +782,12 @@ __device__ __forceinline__ void update_point(const UpdIn<R> &in, UpdOut<R> &out,
   const double kx = (double)ikx, ky = (double)iky, kz = (double)col;
   const bool inm = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
                    col <= g.kcut;
-  const double md = (double)inm * dt;
-  double2 du = cscale(to_d(in.n[0]), md);
-  double2 dv = cscale(to_d(in.n[1]), md);
-  double2 dw = cscale(to_d(in.n[2]), md);
+  // main.c multiplies by the 0/1 mask; N is selected instead, because the
+  // forward passes leave the entries outside the 2/3 rule unwritten
+  const double2 zero = make_double2(0.0, 0.0);
+  double2 du = inm ? cscale(to_d(in.n[0]), dt) : zero;
+  double2 dv = inm ? cscale(to_d(in.n[1]), dt) : zero;
+  double2 dw = inm ? cscale(to_d(in.n[2]), dt) : zero;
   const double kk = kx * kx + ky * ky + kz * kz;
   double2 P;
   if (kk > 0) {
@@ -847,9 +866,13 @@ __global__ void __launch_bounds__(UPD_THREADS)
   const V *vn = (const V *)nl, *vus = (const V *)sa.us, *vz = (const V *)sa.u0,
           *va = (const V *)sa.acc;
   V ln[3], lus[3], lz[3], la[3];
+  // N is read only where some point of the access lies inside the 2/3 rule
+  const int ikx = kwave((int)(row / N), N), iky = kwave((int)(row % N), N);
+  const bool need_n = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
+                      col0 <= g.kcut;
 #pragma unroll
   for (int f = 0; f < 3; f++) {
-    ln[f] = vn[f * vs + vo];
+    ln[f] = need_n ? vn[f * vs + vo] : V{};
     lus[f] = vus[f * vs + vo];
     if (ST == 1 || ST == 2) lz[f] = vz[f * vs + vo];
     if (ST != 0) la[f] = va[f * vs + vo];
