@@ -239,7 +239,11 @@ struct Ops {
   template <int AXIS, bool FWD>
   static void colpass_io(const Group &G, cudaStream_t st, const C *in, C *out, const ColJobs &jobs,
                          int nruns) {
-    dim3 grid(G.g.nfp / CW<AXIS>, N, jobs.njobs * nruns);
+    // a masked pass covers the tiles holding kz <= kcut and, along x, the
+    // ky rows with |ky| <= kcut (kernels.cuh maps them back)
+    const int tiles = jobs.masked ? G.g.kcut / CW<AXIS> + 1 : G.g.nfp / CW<AXIS>;
+    const int rows = (jobs.masked && AXIS == 0) ? 2 * G.g.kcut + 1 : N;
+    dim3 grid(tiles, rows, jobs.njobs * nruns);
     colkern<AXIS, FWD>()<<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
   }
   template <int AXIS, bool FWD>

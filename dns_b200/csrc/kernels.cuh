@@ -53,9 +53,9 @@ struct Geo {
 // to a der slot, in every run of the batch; with an add slot the derivative
 // output is add - i*k*f instead (the same tile of another slot).  A masked
 // pass (the forward passes of N, whose result only enters the update inside
-// the 2/3 rule, main.c:381-386) skips tiles whose kz columns all exceed kcut,
-// in the x pass also ky rows beyond kcut, and stores only |k| <= kcut along
-// its own axis.
+// the 2/3 rule, main.c:381-386) is launched on the column tiles that hold
+// kz <= kcut only, in the x pass also on the ky rows with |ky| <= kcut only,
+// and stores only |k| <= kcut along its own axis.
 struct ColJobs {
   int in_slot[8];
   int out_slot[8];   // -1: no plain output
@@ -118,19 +118,15 @@ __device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R>
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *st = (C *)smem_raw;  // stage twiddles (<= N entries)
   C *xb = st + N;
-  if (jobs.masked) {  // whole block, before any barrier
-    if ((int)blockIdx.x * W > g.kcut) return;
-    if (AXIS == 0) {
-      const int ky = kwave(blockIdx.y, N);
-      if ((ky < 0 ? -ky : ky) > g.kcut) return;
-    }
-  }
   build_stage_tw<N, Plan<N>>(st, twg, N);
   __syncthreads();
   const int p = threadIdx.x % W, t = threadIdx.x / W;
   const int col = blockIdx.x * W + p;
   const bool ok = col < g.nf;
-  const int fixed = blockIdx.y;  // j for the x pass, i for the y pass
+  // j for the x pass, i for the y pass; a masked x pass is launched on the
+  // 2 kcut + 1 rows with |ky| <= kcut only: rows past kcut map to n - kcut..
+  int fixed = blockIdx.y;
+  if (AXIS == 0 && jobs.masked && fixed > g.kcut) fixed += N - (2 * g.kcut + 1);
   const int job = blockIdx.z % jobs.njobs;
   const long long rb = (long long)(blockIdx.z / jobs.njobs) * g.run_spec;
   in += rb;
