@@ -21,14 +21,17 @@
 //   A   x backward  state (3) -> u,v,w and d/dx of v,w            (per field)
 //   B   y backward  5 slots -> u,v,w, omega_z = dv/dx - du/dy, dw/dx, dw/dy
 //   C   z pass      per z line: vorticity from the 6 slots, u and omega to
-//                   real space, N = u x omega, N back to z spectral; real
-//                   space touches HBM only for the stale velocity
-//   D   y forward   3 slots, in place
-//   E1  x forward   3 slots, in place
+//                   real space, N = u x omega, N back to z spectral (stored
+//                   for kz <= kcut); real space touches HBM only for the
+//                   stale velocity
+//   D   y forward   3 slots, in place, tiles with kz <= kcut, |ky| <= kcut kept
+//   E1  x forward   3 slots, in place, rows |ky| <= kcut, |kx| <= kcut kept
 //   E2  update      2/3 mask, projection, viscous term, RK4 updates
 // The vorticity is assembled from spectral derivatives taken on the axis a
 // pass owns (x in A, y in B, z in C), so A, B, D and E1 work on one field per
-// tile and need no cross-field staging.
+// tile and need no cross-field staging.  N only enters the update through
+// the 2/3 rule (main.c:381-386), so C, D and E1 move only those modes and E2
+// reads N there only.
 #pragma once
 #include "fft_core.cuh"
 
