@@ -119,3 +119,27 @@ def test_product_does_not_import_oracle():
             if fn.endswith((".py", ".c", ".cu", ".cuh", ".h")):
                 text = open(os.path.join(dirpath, fn)).read()
                 assert "import oracle" not in text and "liboracle" not in text, fn
+
+
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256, 512])
+def test_bench_mask_fractions_follow_the_two_thirds_rule(n):
+    """bench.py counts the N traffic of the masked forward passes with the
+    mode counts of main.c's mask (|k| < 2/3 (n/2 + 1), main.c:231-238)."""
+    import bench
+
+    kmax = 2.0 / 3.0 * (n // 2 + 1)
+    kz = [k for k in range(n // 2 + 1) if abs(k) < kmax]
+    kxy = [i if i < n // 2 else i - n for i in range(n)]
+    kxy = [k for k in kxy if abs(k) < kmax]
+    fz, fxy = bench.mask_fractions(n)
+    assert fz == len(kz) / (n // 2 + 1)
+    assert fxy == len(kxy) / n
+
+
+def test_bench_step_bytes_256():
+    """Algorithmic bytes of one 256^3 FP64 step (the figure the roofline
+    fields are built on): 25.13 GB with the masked forward passes."""
+    import bench
+
+    total = sum(map(sum, bench.pass_bytes(256)))
+    assert abs(total / 1e9 - 25.13) < 0.01, total
