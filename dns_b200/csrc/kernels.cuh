@@ -820,7 +820,7 @@ __device__ __forceinline__ void update_point(const UpdIn<R> &in, UpdOut<R> &out,
   }
 }
 
-constexpr int UPD_THREADS = 256;
+constexpr int UPD_THREADS = 128;
 // adjacent points per vector access: two float2 make one 16-byte access
 template <class R>
 struct UpdVec;
