@@ -75,6 +75,10 @@ _SIGS = {
     "dns_synchronize": (ctypes.c_int, [_P]),
     "dns_time_kernels": (ctypes.c_int, [_P, _D, _D, ctypes.c_long, ctypes.POINTER(_D)]),
     "dns_diagnostics_noalloc": (ctypes.c_int, [ctypes.c_long, _P, _P, _P]),
+    "dns_set_tgv": (ctypes.c_int, [_P]),
+    "dns_set_perturbed_tgv": (ctypes.c_int, [_P, ctypes.c_ulonglong, _D]),
+    "dns_ens_set_tgv": (ctypes.c_int, [_P, ctypes.c_int]),
+    "dns_ens_set_perturbed_tgv": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_ulonglong, _D]),
     "dns_ens_create": (ctypes.c_int, [ctypes.c_int, _P, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(_P)]),
     "dns_ens_destroy": (ctypes.c_int, [_P]),
     "dns_ens_set_velocity": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
@@ -159,19 +163,32 @@ class Context:
                 raise ValueError("velocity component must have n^3 values")
         _check(self._lib.dns_set_velocity(self._h, _ptr(U), _ptr(V), _ptr(W)))
 
+    def set_tgv(self) -> None:
+        """Taylor-Green of tgv.py generated on the device (dns_set_tgv)."""
+        _check(self._lib.dns_set_tgv(self._h))
+
+    def set_perturbed_tgv(self, seed: int, amplitude: float = 1e-3) -> None:
+        """Taylor-Green plus the seeded solenoidal perturbation of
+        perturbed_tgv(..., rng="counter"), generated on the device."""
+        _check(self._lib.dns_set_perturbed_tgv(self._h, seed, amplitude))
+
     def step(self, nu: float, dt: float, nsteps: int = 1) -> None:
         _check(self._lib.dns_step(self._h, nu, dt, nsteps))
 
-    def diagnostics_dd(self) -> Tuple[float, float, float, float]:
+    def diagnostics_dd(self, allow_nonfinite: bool = False) -> Tuple[float, float, float, float]:
+        """Double-double sums (e_hi, e_lo, om_hi, om_lo) of dns_diagnostics.
+        A NaN or Inf raises DNSError (DNS_ERR_NONFINITE), as main.c stops on
+        the first non-finite value (main.c:49-50); allow_nonfinite=True
+        returns the raw values instead."""
         v = [ctypes.c_double() for _ in range(4)]
         st = self._lib.dns_diagnostics(self._h, *[ctypes.byref(x) for x in v])
-        if st not in (DNS_OK, DNS_ERR_NONFINITE):
+        if st != DNS_OK and not (allow_nonfinite and st == DNS_ERR_NONFINITE):
             _check(st)
         return tuple(x.value for x in v)
 
-    def diagnostics(self) -> Tuple[np.longdouble, np.longdouble]:
+    def diagnostics(self, allow_nonfinite: bool = False) -> Tuple[np.longdouble, np.longdouble]:
         """Energy and enstrophy exactly as main.c:257-266 prints them."""
-        eh, el, oh, ol = self.diagnostics_dd()
+        eh, el, oh, ol = self.diagnostics_dd(allow_nonfinite)
         return scale_diagnostics(eh, el, oh, ol, self.n)
 
     def get_fields(self, pressure: bool = False):
@@ -254,6 +271,12 @@ class Ensemble:
         U, V, W = _f64(U), _f64(V), _f64(W)
         _check(self._lib.dns_ens_set_velocity(self._h, run, _ptr(U), _ptr(V), _ptr(W)))
 
+    def set_tgv(self, run: int) -> None:
+        _check(self._lib.dns_ens_set_tgv(self._h, run))
+
+    def set_perturbed_tgv(self, run: int, seed: int, amplitude: float = 1e-3) -> None:
+        _check(self._lib.dns_ens_set_perturbed_tgv(self._h, run, seed, amplitude))
+
     def set_params(self, nu, dt) -> None:
         nu = _f64(np.broadcast_to(np.asarray(nu, dtype=np.float64), (len(self.sizes),)))
         dt = _f64(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.sizes),)))
@@ -262,11 +285,12 @@ class Ensemble:
     def step(self, nsteps: int = 1) -> None:
         _check(self._lib.dns_ens_step(self._h, nsteps))
 
-    def diagnostics(self):
-        """Per run (E, Omega) as main.c prints them."""
+    def diagnostics(self, allow_nonfinite: bool = False):
+        """Per run (E, Omega) as main.c prints them.  A NaN or Inf in any run
+        raises DNSError unless allow_nonfinite=True."""
         out = np.empty(4 * len(self.sizes))
         st = self._lib.dns_ens_diagnostics(self._h, _ptr(out))
-        if st not in (DNS_OK, DNS_ERR_NONFINITE):
+        if st != DNS_OK and not (allow_nonfinite and st == DNS_ERR_NONFINITE):
             _check(st)
         return [scale_diagnostics(*out[4 * r:4 * r + 4], n) for r, n in enumerate(self.sizes)]
 
@@ -284,12 +308,50 @@ class Ensemble:
         _check(self._lib.dns_ens_synchronize(self._h))
 
 
-def solenoidal_perturbation(n: int, seed: int, k0: float = 4.0):
+_M64 = (1 << 64) - 1
+_GOLDEN64 = 0x9E3779B97F4A7C15
+
+
+def _mix64(z):
+    """SplitMix64 output function on uint64 arrays (wrapping arithmetic)."""
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def counter_normals(seed: int, field: int, count: int) -> np.ndarray:
+    """Standard normal numbers 0..count-1 of stream `field` of `seed`, from the
+    counter-based generator the device uses (dns_b200/csrc/init.cuh):
+    SplitMix64's output function of key + (i + 1) * golden, two 53-bit
+    uniforms per number, Box-Muller (cosine branch)."""
+    key = int(_mix64(np.array([((seed * _GOLDEN64) + field + 1) & _M64], dtype=np.uint64))[0])
+    out = np.empty(count)
+    chunk = 1 << 22
+    for a0 in range(0, count, chunk):
+        i = np.arange(a0, min(count, a0 + chunk), dtype=np.uint64)
+        with np.errstate(over="ignore"):
+            a = _mix64(np.uint64(key) + (np.uint64(2) * i + np.uint64(1)) * np.uint64(_GOLDEN64))
+            b = _mix64(np.uint64(key) + (np.uint64(2) * i + np.uint64(2)) * np.uint64(_GOLDEN64))
+        u1 = ((a >> np.uint64(11)) + np.uint64(1)).astype(np.float64) * 2.0 ** -53
+        u2 = (b >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+        out[a0:a0 + len(i)] = np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+    return out
+
+
+def solenoidal_perturbation(n: int, seed: int, k0: float = 4.0, rng: str = "pcg64"):
     """Seeded random divergence-free velocity with energy spectrum
-    E(k) ~ k^4 exp(-2 (k/k0)^2): white Gaussian noise (numpy PCG64(seed)),
-    forward transform, amplitude sqrt(E(k)) / k per mode, projection onto
-    k-perpendicular, back transform.  Returned with unit rms."""
-    rng = np.random.Generator(np.random.PCG64(seed))
+    E(k) ~ k^4 exp(-2 (k/k0)^2): white Gaussian noise, forward transform,
+    amplitude sqrt(E(k)) / k per mode, projection onto k-perpendicular, back
+    transform.  Returned with unit rms.  rng="pcg64": the noise of numpy's
+    PCG64(seed); rng="counter": the device's counter-based generator
+    (counter_normals), the stream dns_set_perturbed_tgv draws with k0 = 4."""
+    if rng == "pcg64":
+        gen = np.random.Generator(np.random.PCG64(seed))
+        noise = [gen.standard_normal((n, n, n)) for _ in range(3)]
+    elif rng == "counter":
+        noise = [counter_normals(seed, f, n ** 3).reshape(n, n, n) for f in range(3)]
+    else:
+        raise ValueError(f"unknown rng {rng!r}")
     k1 = np.fft.fftfreq(n, 1.0 / n)
     kz = np.arange(n // 2 + 1, dtype=np.float64)
     KX, KY, KZ = np.meshgrid(k1, k1, kz, indexing="ij")
@@ -299,7 +361,7 @@ def solenoidal_perturbation(n: int, seed: int, k0: float = 4.0):
     # no Nyquist content (its derivative is ambiguous on the half spectrum)
     nyq = (np.abs(KX) == n // 2) | (np.abs(KY) == n // 2) | (KZ == n // 2)
     amp[nyq] = 0.0
-    hats = [np.fft.rfftn(rng.standard_normal((n, n, n))) * amp for _ in range(3)]
+    hats = [np.fft.rfftn(x) * amp for x in noise]
     div = (KX * hats[0] + KY * hats[1] + KZ * hats[2]) / np.where(kk > 0, kk, 1.0)
     hats = [hats[0] - KX * div, hats[1] - KY * div, hats[2] - KZ * div]
     u = [np.fft.irfftn(h, s=(n, n, n), axes=(0, 1, 2)) for h in hats]
@@ -307,13 +369,13 @@ def solenoidal_perturbation(n: int, seed: int, k0: float = 4.0):
     return [c / rms for c in u]
 
 
-def perturbed_tgv(n: int, seed: int, amplitude: float = 1e-3):
+def perturbed_tgv(n: int, seed: int, amplitude: float = 1e-3, rng: str = "pcg64"):
     """Taylor-Green plus a seeded solenoidal perturbation whose rms is
     `amplitude` times the rms of the Taylor-Green field (the ensemble
-    configuration's initial fields)."""
+    configuration's initial fields; rng as in solenoidal_perturbation)."""
     U, V, W, _ = tgv_fields(n)
     rms_tgv = np.sqrt(np.mean(U ** 2 + V ** 2 + W ** 2))
-    d = solenoidal_perturbation(n, seed)
+    d = solenoidal_perturbation(n, seed, rng=rng)
     s = amplitude * rms_tgv
     return U + s * d[0], V + s * d[1], W + s * d[2]
 

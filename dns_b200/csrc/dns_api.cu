@@ -17,6 +17,7 @@
 // main.c:415-420 disappear.
 #include "dns_b200.h"
 #include "adjoint.cuh"
+#include "init.cuh"
 #include "kernels.cuh"
 
 #include <math.h>
@@ -192,6 +193,7 @@ ColJobs jobs_map(const int *in, const int *out, int cnt) {
 
 template <class R, int N>
 struct Ops {
+  using Real = R;
   using C = cx<R>;
   static constexpr int Nval = N;
   static constexpr int E = Plan<N>::E;
@@ -526,6 +528,79 @@ int set_velocity_view(const Group &V, cudaStream_t st, const double *U, const do
   return DNS_OK;
 }
 
+// 1-D tables of tgv.py:16-22: s_i = sin(i dx), c_i = cos(i dx) with
+// dx = 2 pi / n in double (the C library's sin and cos)
+void tgv_tables(long n, std::vector<double> &tab) {
+  const double dx = 2 * 3.141592653589793 / (double)n;
+  tab.resize(2 * n);
+  for (long i = 0; i < n; i++) {
+    tab[i] = sin(dx * (double)i);
+    tab[n + i] = cos(dx * (double)i);
+  }
+}
+
+// Taylor-Green of tgv.py (plus, with `perturb`, the seeded solenoidal
+// perturbation of init.cuh) generated on the device into the stale slots of
+// run `run` of G, then transformed like dns_set_velocity.  The perturbation
+// is shaped at the storage precision (float32 FFTs in a mixed group).
+int init_view(Group &G, int run, cudaStream_t st, bool perturb, unsigned long long seed,
+              double amplitude) {
+  const Group V = G.one(run);
+  const Geo &g = V.g;
+  const long n = G.n;
+  const bool fp64 = G.precision == DNS_PREC_FP64;
+  std::vector<double> tab;
+  tgv_tables(n, tab);
+  double *dtab = (double *)V.slot_ptr(0, SLOT_WORK + 6);  // free until the forward transform
+  CK(cudaMemcpyAsync(dtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  double *delta = nullptr;
+  double rms = 1.0, scale = 0.0;
+  const unsigned blocks = conv_blocks(3 * g.nreal);
+  if (perturb) {
+    if (!fp64 && !G.realbuf) CK(cudaMalloc((void **)&G.realbuf, 4 * (size_t)g.nreal * sizeof(double)));
+    // FP64: the stale slots hold the noise until its forward transform, then
+    // the shaped field; mixed: a float64 buffer
+    delta = fp64 ? (double *)V.stale : G.realbuf;
+    dispatch(V, [&](auto ops) {
+      using O = decltype(ops);
+      using R = typename O::Real;
+      k_noise3<R><<<blocks, 256, 0, st>>>((R *)V.stale, g.nreal, seed);
+      O::forward(V, st);
+      k_shape_project<typename O::C><<<conv_blocks((long long)n * n * g.nf), 256, 0, st>>>(
+          O::slot(V, SLOT_SA), g, 4.0);
+      const int f3[3] = {0, 1, 2};
+      O::c2r_fields(V, st, O::slot(V, SLOT_SA), f3, 3, delta, 1.0 / (double)g.nreal);
+    });
+    k_sumsq<256><<<V.diag_blocks, 256, 0, st>>>(delta, 3 * g.nreal, V.diag_part);
+    k_diag_final<256><<<1, 256, 0, st>>>(V.diag_part, V.diag_blocks, V.diag_out);
+    CKL();
+    double4 sum;
+    CK(cudaMemcpyAsync(&sum, V.diag_out, sizeof sum, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    rms = sqrt((sum.x + sum.y) / (double)g.nreal);
+    // rms of the Taylor-Green field: mean of U^2 + V^2 = 2 S C^2 / n^3 with
+    // S = sum s_i^2, C = sum c_i^2
+    long double S = 0, Cs = 0;
+    for (long i = 0; i < n; i++) {
+      S += (long double)tab[i] * tab[i];
+      Cs += (long double)tab[n + i] * tab[n + i];
+    }
+    const double rms_tgv = (double)sqrtl(2.0L * S * Cs * Cs / ((long double)n * n * n));
+    scale = amplitude * rms_tgv;
+    if (!(rms > 0) || !isfinite(rms))
+      return fail(DNS_ERR_NONFINITE, "perturbation has no energy", __FILE__, __LINE__);
+  }
+  dispatch(V, [&](auto ops) {
+    using O = decltype(ops);
+    using R = typename O::Real;
+    k_tgv_fill<R><<<blocks, 256, 0, st>>>((R *)V.stale, dtab, delta, rms, scale, (int)n);
+    O::forward(V, st);
+  });
+  CKL();
+  CK(cudaStreamSynchronize(st));
+  return DNS_OK;
+}
+
 int get_spectral_view(const Group &V, cudaStream_t st, double *uvw) {
   const Geo &g = V.g;
   const size_t row = (size_t)g.nf * sizeof(double2);
@@ -853,6 +928,20 @@ int dns_diagnostics(dns_ctx *c, double *e_hi, double *e_lo, double *om_hi, doubl
   return DNS_OK;
 }
 
+int dns_set_tgv(dns_ctx *c) {
+  if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
+  int st = init_view(c->grp, 0, c->stream, false, 0, 0.0);
+  if (st == DNS_OK) c->have_state = true;
+  return st;
+}
+
+int dns_set_perturbed_tgv(dns_ctx *c, unsigned long long seed, double amplitude) {
+  if (!c || !isfinite(amplitude)) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  int st = init_view(c->grp, 0, c->stream, true, seed, amplitude);
+  if (st == DNS_OK) c->have_state = true;
+  return st;
+}
+
 int dns_get_fields(dns_ctx *c, double *U, double *V, double *W, double *P) {
   if (!c) return fail(DNS_ERR_ARG, "NULL context", __FILE__, __LINE__);
   Group &G = c->grp;
@@ -939,7 +1028,16 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
     c->cur_dt = dt;
   }
   const int K = c->kernels_per_step;
-  std::vector<cudaEvent_t> ev(K + 1);
+  // destroyed on every return path, the early ones of CK included
+  struct Events {
+    std::vector<cudaEvent_t> v;
+    ~Events() {
+      for (cudaEvent_t e : v)
+        if (e) cudaEventDestroy(e);
+    }
+  } evs;
+  evs.v.assign(K + 1, nullptr);
+  std::vector<cudaEvent_t> &ev = evs.v;
   for (auto &e : ev) CK(cudaEventCreate(&e));
   for (int k = 0; k < K; k++) ms[k] = 0.0;
   int st = DNS_OK;
@@ -959,7 +1057,6 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
       ms[k] += t;
     }
   }
-  for (auto &e : ev) cudaEventDestroy(e);
   for (int k = 0; k < K; k++) ms[k] /= (double)nsteps;
   return st;
 }
@@ -1042,6 +1139,23 @@ int dns_ens_set_velocity(dns_ens *e, int run, const double *U, const double *V, 
   if (!U || !V || !W) return fail(DNS_ERR_ARG, "NULL argument", __FILE__, __LINE__);
   const Group view = e->groups[e->run_group[run]].one(e->run_index[run]);
   st = set_velocity_view(view, e->stream, U, V, W);
+  if (st == DNS_OK) e->have_state[run] = 1;
+  return st;
+}
+
+int dns_ens_set_tgv(dns_ens *e, int run) {
+  int st = ens_check_run(e, run);
+  if (st != DNS_OK) return st;
+  st = init_view(e->groups[e->run_group[run]], e->run_index[run], e->stream, false, 0, 0.0);
+  if (st == DNS_OK) e->have_state[run] = 1;
+  return st;
+}
+
+int dns_ens_set_perturbed_tgv(dns_ens *e, int run, unsigned long long seed, double amplitude) {
+  int st = ens_check_run(e, run);
+  if (st != DNS_OK) return st;
+  if (!isfinite(amplitude)) return fail(DNS_ERR_ARG, "bad amplitude", __FILE__, __LINE__);
+  st = init_view(e->groups[e->run_group[run]], e->run_index[run], e->stream, true, seed, amplitude);
   if (st == DNS_OK) e->have_state[run] = 1;
   return st;
 }

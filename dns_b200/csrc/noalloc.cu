@@ -19,6 +19,8 @@
 #include "dns_b200.h"
 #include "kernels.cuh"
 
+#include <cuda.h>  // CUcontext / CUresult types only; the driver is reached through the runtime
+
 #include <mutex>
 #include <stdio.h>
 
@@ -34,16 +36,82 @@ constexpr int NOALLOC_THREADS = 256;
 constexpr int NOALLOC_PER_THREAD = 32;
 constexpr long long NOALLOC_CHUNK = (long long)NOALLOC_THREADS * NOALLOC_PER_THREAD;  // 8192
 constexpr int NOALLOC_MAX_PARTIALS = 8224;  // = ceil(512^2 * 257 / NOALLOC_CHUNK)
+static_assert((long long)NOALLOC_MAX_PARTIALS * NOALLOC_CHUNK >= 512LL * 512 * 257,
+              "the scratch must hold one partial per block of the n = 512 grid");
 
 // Shared by every call on a device.  Every block of a call writes its own
 // entry before the final block reads it, so nothing has to start at zero; two
 // calls that overlap on the GPU (different streams, no ordering) race on it.
 __device__ __align__(256) double4 g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 
-// device address of g_noalloc_partials, looked up once per device
-constexpr int MAX_DEVICES = 64;
-double4 *g_partials_addr[MAX_DEVICES] = {};
+// Device address of g_noalloc_partials, looked up once per CUDA context and
+// cached under the context's unique id (cuCtxGetId).  Keying on the device
+// index alone would go wrong after cudaDeviceReset, or under a driver-API
+// context other than the device's primary one: the array then lives at a new
+// address, and the cached one would point into freed or foreign memory.
+// Context ids are never reused within a process.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+constexpr int ADDR_CACHE = 64;
+struct AddrEntry {
+  unsigned long long ctx_id;
+  double4 *addr;
+};
+AddrEntry g_addr_cache[ADDR_CACHE] = {};
+int g_addr_next = 0;
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
 std::mutex g_setup_mutex;
+
+// id of the calling thread's current context (0: none current yet)
+cudaError_t current_ctx_id(unsigned long long *id) {
+  *id = 0;
+  if (!g_ctx_get_current) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e != cudaSuccess) return e;
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return cudaErrorNotSupported;
+    g_ctx_get_id = (PfnCtxGetId)f2;
+    g_ctx_get_current = (PfnCtxGetCurrent)f1;
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return cudaErrorUnknown;
+  if (ctx && g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return cudaErrorUnknown;
+  return cudaSuccess;
+}
+
+// the scratch's device address in the current context (set-up on the first
+// call in a context: the symbol lookup, which also loads this file's module)
+cudaError_t partials_address(double4 **out) {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  unsigned long long id = 0;
+  cudaError_t e = current_ctx_id(&id);
+  if (e != cudaSuccess) return e;
+  if (id) {
+    for (const AddrEntry &a : g_addr_cache)
+      if (a.ctx_id == id && a.addr) {
+        *out = a.addr;
+        return cudaSuccess;
+      }
+  }
+  // host code only holds a stand-in for the array: ask for its device address
+  void *p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+  if (e != cudaSuccess) return e;
+  if (!id) {  // the lookup made the device's primary context current
+    e = current_ctx_id(&id);
+    if (e != cudaSuccess) return e;
+  }
+  if (id) {
+    g_addr_cache[g_addr_next] = AddrEntry{id, (double4 *)p};
+    g_addr_next = (g_addr_next + 1) % ADDR_CACHE;
+  }
+  *out = (double4 *)p;
+  return cudaSuccess;
+}
 
 // Same terms and double-double arithmetic as k_diag, but each block reduces
 // the fixed chunk [blockIdx.x * NOALLOC_CHUNK, +NOALLOC_CHUNK) of points of an
@@ -90,32 +158,24 @@ extern "C" int dns_diagnostics_noalloc(long n, const double *uvw_hat, double *ou
                         "dns_diagnostics_noalloc: input larger than the fixed scratch "
                         "(n^2 (n/2+1) must be <= 67371008 points, n <= 512)");
   if (!uvw_hat || !out) return noalloc_fail(DNS_ERR_ARG, "dns_diagnostics_noalloc: NULL pointer");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
-  if (dev < 0 || dev >= MAX_DEVICES)
-    return noalloc_fail(DNS_ERR_UNSUPPORTED, "dns_diagnostics_noalloc: device index too large");
   double4 *partials = nullptr;
-  {
-    // set-up, once per device, with that device current: the host-side name
-    // g_noalloc_partials is only a stand-in, the kernel needs the device
-    // address.  This first call on a device also loads the module, so it
-    // should happen before any stream capture.
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-      if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
-      g_partials_addr[dev] = (double4 *)p;
-    }
-    partials = g_partials_addr[dev];
-  }
+  cudaError_t e = partials_address(&partials);
+  if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+  // each launch's own status (cudaLaunchKernel), so that an error left
+  // pending by the caller's earlier, unrelated work is neither reported as
+  // this call's failure nor cleared
   cudaStream_t s = (cudaStream_t)stream;
-  k_diag_chunk<<<(unsigned)nblocks, NOALLOC_THREADS, 0, s>>>((const cd *)uvw_hat, (int)n, npts,
-                                                            partials);
-  k_diag_final<NOALLOC_THREADS><<<1, NOALLOC_THREADS, 0, s>>>(partials, (int)nblocks,
-                                                              (double4 *)out);
-  e = cudaGetLastError();
+  const cd *u = (const cd *)uvw_hat;
+  int ni = (int)n, nb = (int)nblocks;
+  long long np = npts;
+  double4 *res = (double4 *)out;
+  void *a1[] = {(void *)&u, (void *)&ni, (void *)&np, (void *)&partials};
+  e = cudaLaunchKernel((const void *)k_diag_chunk, dim3((unsigned)nblocks), dim3(NOALLOC_THREADS),
+                       a1, 0, s);
+  if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+  void *a2[] = {(void *)&partials, (void *)&nb, (void *)&res};
+  e = cudaLaunchKernel((const void *)k_diag_final<NOALLOC_THREADS>, dim3(1), dim3(NOALLOC_THREADS),
+                       a2, 0, s);
   if (e != cudaSuccess) return noalloc_fail(DNS_ERR_CUDA, cudaGetErrorString(e));
   return DNS_OK;
 }

@@ -91,6 +91,25 @@ int dns_diagnostics(dns_ctx *ctx, double *e_hi, double *e_lo, double *om_hi, dou
  * Replaces the dump transform of main.c:270-279. */
 int dns_get_fields(dns_ctx *ctx, double *U, double *V, double *W, double *P);
 
+/* Initial velocity generated on the device, with no n^3 host transfer; the
+ * field also becomes the stale real-space velocity of step 0, exactly as
+ * after dns_set_velocity.
+ *
+ * dns_set_tgv: the Taylor-Green field tgv.py writes (tgv.py:14-27),
+ *   U = sin x cos y cos z, V = -cos x sin y cos z, W = 0 at x_i = i 2 pi / n,
+ *   bit-identical to tgv.py's .raw (same 1-D sin/cos tables, same order of
+ *   the products).  Replaces `python tgv.py -l L -o f.raw` + main.c:163-185
+ *   + main.c:249-251.
+ * dns_set_perturbed_tgv: the same plus a seeded solenoidal perturbation with
+ *   energy spectrum E(k) ~ k^4 exp(-2 (k/4)^2) and rms = amplitude times the
+ *   rms of the Taylor-Green field (white Gaussian noise from a counter-based
+ *   generator keyed by seed, r2c, shaped and projected per mode, c2r, scaled
+ *   to unit rms).  No counterpart in the reference; it is the initial field
+ *   of the ensemble configuration.  In a DNS_PREC_MIXED context the
+ *   perturbation is shaped with float32 transforms. */
+int dns_set_tgv(dns_ctx *ctx);
+int dns_set_perturbed_tgv(dns_ctx *ctx, unsigned long long seed, double amplitude);
+
 /* Human-readable text of a status / of the last error on this thread. */
 const char *dns_strerror(int status);
 const char *dns_last_error(void);
@@ -144,6 +163,10 @@ int dns_ens_create(int nruns, const long *n, int precision, unsigned flags, dns_
 int dns_ens_destroy(dns_ens *e);
 /* initial velocity of one run (as dns_set_velocity) */
 int dns_ens_set_velocity(dns_ens *e, int run, const double *U, const double *V, const double *W);
+/* initial velocity of one run generated on the device (as dns_set_tgv /
+ * dns_set_perturbed_tgv) */
+int dns_ens_set_tgv(dns_ens *e, int run);
+int dns_ens_set_perturbed_tgv(dns_ens *e, int run, unsigned long long seed, double amplitude);
 /* viscosity and time step of every run (arrays of nruns) */
 int dns_ens_set_params(dns_ens *e, const double *nu, const double *dt);
 /* advance every run by nsteps RK4 steps */
@@ -188,8 +211,10 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
  * Scratch is a fixed 263 KB device array inside the library (every GPU that
  * loads the library holds it until exit), sized for the n = 512 grid: larger
  * inputs (more than 67,371,008 half-spectrum points) are rejected with
- * DNS_ERR_UNSUPPORTED, as is any n outside the range.  The first call on a device looks up that array's device
- * address and loads the kernels, so make it before any stream capture.
+ * DNS_ERR_UNSUPPORTED, as is any n outside the range.  The first call in a
+ * CUDA context (on each device, and again after cudaDeviceReset or under
+ * another context) looks up that array's device address and loads the
+ * kernels, so make it before any stream capture.
  * Every call shares the array: calls that can overlap on the GPU (different
  * streams without ordering, or different host threads on one device) race;
  * serialise them.  Nothing in it has to start at zero (each call overwrites

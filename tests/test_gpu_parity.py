@@ -297,7 +297,10 @@ def test_nonfinite_is_reported(dns):
     U[3, 4, 5] = np.nan
     with dns.Context(n) as ctx:
         ctx.set_velocity(U, V, W)
-        eh, el, oh, ol = ctx.diagnostics_dd()
+        with pytest.raises(dns.DNSError) as e:
+            ctx.diagnostics()
+        assert e.value.status == dns.DNS_ERR_NONFINITE
+        eh, el, oh, ol = ctx.diagnostics_dd(allow_nonfinite=True)
         assert np.isnan(eh)
         st = ctx._lib.dns_diagnostics(ctx._h, None, None, None, None)
         assert st == dns.DNS_ERR_NONFINITE

@@ -143,3 +143,40 @@ def test_bench_step_bytes_256():
 
     total = sum(map(sum, bench.pass_bytes(256)))
     assert abs(total / 1e9 - 25.13) < 0.01, total
+
+
+def _scalar_counter_normal(seed, field, i):
+    """Pure-Python restatement of the counter-based generator (SplitMix64
+    output function, Box-Muller), one number at a time."""
+    import math
+
+    m = (1 << 64) - 1
+    g = 0x9E3779B97F4A7C15
+
+    def mix(z):
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        return z ^ (z >> 31)
+
+    key = mix((seed * g + field + 1) & m)
+    a = mix((key + (2 * i + 1) * g) & m)
+    b = mix((key + (2 * i + 2) * g) & m)
+    u1 = ((a >> 11) + 1) * 2.0 ** -53
+    u2 = (b >> 11) * 2.0 ** -53
+    return math.sqrt(-2.0 * math.log(u1)) * math.cos(6.283185307179586 * u2)
+
+
+def test_counter_normals_match_scalar_restatement_and_are_normal():
+    """The numpy form of the device's noise generator (used as the host
+    reference of dns_set_perturbed_tgv) against a scalar restatement, and
+    its first two moments."""
+    import dns_b200
+
+    for seed, field in ((0, 0), (12345, 2), (2 ** 63 + 7, 1)):
+        x = dns_b200.counter_normals(seed, field, 1 << 12)
+        for i in (0, 1, 2, 1000, 4095):
+            assert x[i] == pytest.approx(_scalar_counter_normal(seed, field, i), rel=1e-15, abs=1e-15)
+    x = dns_b200.counter_normals(3, 0, 1 << 20)
+    assert abs(x.mean()) < 5e-3 and abs(x.std() - 1) < 5e-3
+    assert np.array_equal(x[:100], dns_b200.counter_normals(3, 0, 100))  # a counter, not a state
+    assert not np.allclose(x[:100], dns_b200.counter_normals(3, 1, 100))
