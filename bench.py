@@ -87,16 +87,23 @@ def pass_units(n: int, pressure: bool = False):
     return u
 
 
-def pass_bytes(n: int):
-    cf = n * n * (n // 2 + 1) * 16
-    rf = n ** 3 * 8
+def pass_bytes(n: int, s: int = 8):
+    """Algorithmic bytes of every pass of every stage, s bytes per real
+    (8: FP64, 4: the mixed path's FP32 storage)."""
+    cf = n * n * (n // 2 + 1) * 2 * s
+    rf = n ** 3 * s
     return [[uc * cf + ur * rf for (uc, ur) in st] for st in pass_units(n)]
 
 
-def step_bytes_model(n: int) -> int:
-    """B_step = 216 * n^2 (n/2 + 1) * 2 * 8 bytes: the minimal fused five-pass
+def step_bytes(n: int, s: int = 8) -> int:
+    """Algorithmic bytes of one RK4 step of this implementation."""
+    return int(sum(map(sum, pass_bytes(n, s))))
+
+
+def step_bytes_model(n: int, s: int = 8) -> int:
+    """B_step = 216 * n^2 (n/2 + 1) * 2 * s bytes: the minimal fused five-pass
     traffic model of the reference path (for the % of HBM roofline figure)."""
-    return 216 * n * n * (n // 2 + 1) * 2 * 8
+    return 216 * n * n * (n // 2 + 1) * 2 * s
 
 
 def load_peak():
@@ -248,14 +255,12 @@ def ensemble_leg(steps: int, warmup: int):
     rng = np.random.Generator(np.random.PCG64(2024))
     nus = np.exp(rng.uniform(np.log(1 / 3000), np.log(1 / 100), len(sizes)))
     dt = 0.005
-    fields = {}
-    for r, n in enumerate(sizes):
-        fields[r] = dns_b200.perturbed_tgv(n, seed=r, amplitude=1e-3)
     prec = dns_b200.DNS_PREC_MIXED
     with dns_b200.Ensemble(sizes, prec) as ens:
         st = torch.cuda.ExternalStream(ens.stream)
+        # initial fields generated on the device (seed = run index)
         for r in range(len(sizes)):
-            ens.set_velocity(r, *fields[r])
+            ens.set_perturbed_tgv(r, seed=r, amplitude=1e-3)
         ens.set_params(nus, dt)
         ens.step(warmup)
         ens.synchronize()
@@ -273,7 +278,7 @@ def ensemble_leg(steps: int, warmup: int):
         with dns_b200.Context(n, prec) as c:
             sc = torch.cuda.ExternalStream(c.stream)
             r = sizes.index(n)
-            c.set_velocity(*fields[r])
+            c.set_perturbed_tgv(seed=r, amplitude=1e-3)
             c.step(float(nus[r]), dt, warmup)
             c.synchronize()
             a = torch.cuda.Event(enable_timing=True)
@@ -285,11 +290,87 @@ def ensemble_leg(steps: int, warmup: int):
             seq_ms[n] = a.elapsed_time(b) / steps
     agg = len(sizes) * steps / (ms / 1000.0)
     seq = len(sizes) / ((32 * seq_ms[64] + 16 * seq_ms[128]) / 1000.0)
+    peak, peak_kind = load_peak()
+    ens_bytes = sum(step_bytes(n, 4) for n in sizes)
+    ens_model = sum(step_bytes_model(n, 4) for n in sizes)
+    ens_sps = steps / (ms / 1000.0)
     return {"runs": len(sizes), "sizes": "32x64^3 + 16x128^3", "precision": "mixed",
+            "init": "device (dns_ens_set_perturbed_tgv, seed = run index)",
             "steps": steps, "value": agg, "unit": "run-steps/s",
             "ms_per_ensemble_step": ms / steps, "sequential_value": seq,
             "vs_sequential": agg / seq, "all_finite": finite,
-            "seq_ms_per_step": {str(k): v for k, v in seq_ms.items()}}
+            "seq_ms_per_step": {str(k): v for k, v in seq_ms.items()},
+            "bytes_per_ensemble_step": ens_bytes,
+            "roofline_frac": ens_bytes * ens_sps / (peak * 1e9),
+            "frac_of_model_roofline": ens_model * ens_sps / (peak * 1e9),
+            "peak_source": peak_kind}
+
+
+def n512_leg(steps: int, warmup: int):
+    """512^3 Taylor-Green (generated on the device), nu = 1/3000,
+    dt = 0.0025: FP64 and mixed steps/s and the step's fraction of the
+    measured HBM peak (this implementation's algorithmic bytes, and the
+    216 C model)."""
+    import torch
+
+    import dns_b200
+
+    n = 512
+    peak, _ = load_peak()
+    out = {}
+    for name, prec, s in (("fp64", dns_b200.DNS_PREC_FP64, 8), ("mixed", dns_b200.DNS_PREC_MIXED, 4)):
+        with dns_b200.Context(n, prec) as c:
+            st = torch.cuda.ExternalStream(c.stream)
+            c.set_tgv()
+            c.step(NU, DT, warmup)
+            c.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            c.step(NU, DT, steps)
+            b.record(st)
+            b.synchronize()
+            ms = a.elapsed_time(b) / steps
+        sps = 1000.0 / ms
+        out[name] = {"value": sps, "unit": "steps/s", "ms_per_step": ms, "steps": steps,
+                     "frac": step_bytes(n, s) * sps / (peak * 1e9),
+                     "frac_of_model_roofline": step_bytes_model(n, s) * sps / (peak * 1e9)}
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def adjoint_leg(n: int = 128, snapshots: int = 20):
+    """Discrete adjoint of the final energy (dns_adjoint_energy): 128^3
+    unit-energy random isotropic field, nu = 0.005, dt = 0.005, T = 2
+    (401 steps), 20 snapshots.  Wall time of the whole call (forward sweep
+    with checkpoints, reverse sweep with recomputation, host copies of the
+    field and the gradient) per step, against the plain forward step."""
+    import numpy as np
+
+    import dns_b200
+
+    nu, dt = 0.005, 0.005
+    _, nsteps = dns_b200.step_schedule(2.0, dt)
+    u0 = dns_b200.solenoidal_perturbation(n, seed=0)
+    with dns_b200.Context(n) as c:
+        c.set_velocity(*u0)
+        E0, _ = c.diagnostics()
+        s = float(1.0 / np.sqrt(E0))
+        u0 = [a * s for a in u0]
+        c.set_velocity(*u0)
+        c.step(nu, dt, 5)
+        c.synchronize()
+        t0 = time.perf_counter()
+        c.step(nu, dt, nsteps)
+        c.synchronize()
+        fwd_ms = (time.perf_counter() - t0) * 1000.0 / nsteps
+    dns_b200.adjoint_energy(*u0, nu, dt, 8, snapshots=4)  # warm-up (module load, plans)
+    t0 = time.perf_counter()
+    dns_b200.adjoint_energy(*u0, nu, dt, nsteps, snapshots=snapshots)
+    wall = time.perf_counter() - t0
+    return {"n": n, "steps": nsteps, "snapshots": snapshots, "wall_s": wall,
+            "ms_per_step": wall * 1000.0 / nsteps, "forward_ms_per_step": fwd_ms,
+            "vs_forward_step": wall * 1000.0 / nsteps / fwd_ms}
 
 
 def run_reference_arm(args, world, rank):
@@ -319,6 +400,8 @@ def main() -> int:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-n512", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -393,7 +476,7 @@ def main() -> int:
         traffic = tj.get(str(n), {}).get(dns_b200.PASS_NAMES[dom])
     except Exception:
         pass
-    step_bytes = sum(map(sum, pb))
+    sbytes = step_bytes(n)
 
     # -- mixed precision (FP32 fields/FFTs, FP64 reductions/coefficients) --
     E64, O64 = ctx.diagnostics()  # after warmup + timed + 3 kernel-timing steps
@@ -424,7 +507,8 @@ def main() -> int:
         "energy_rel_err_vs_fp64": float(abs(E32 - E64) / E64),
         "enstrophy_rel_err_vs_fp64": float(abs(O32 - O64) / O64),
         "compared_after_steps": done64,
-        "step_hbm_frac_of_model_roofline": step_bytes_model(n) / 2 * mixed_sps / (peak * 1e9),
+        "step_hbm_frac": step_bytes(n, 4) * mixed_sps / (peak * 1e9),
+        "step_hbm_frac_of_model_roofline": step_bytes_model(n, 4) * mixed_sps / (peak * 1e9),
         "kernel_ms": {dns_b200.PASS_NAMES[p]: [float(mkms[s, p]) for s in range(4)] for p in range(K)},
     }
 
@@ -467,6 +551,8 @@ def main() -> int:
     d2h = (3 * n ** 3 * 8 + 32 * ndiag) / args.steps
 
     ens = ensemble_leg(500, args.warmup) if not args.no_ensemble else None
+    big = n512_leg(20, 3) if (n == 256 and not args.no_n512) else None
+    adj = adjoint_leg() if (n == 256 and not args.no_adjoint) else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -499,7 +585,8 @@ def main() -> int:
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": dns_b200.PASS_NAMES[dom], "peak_source": peak_kind,
                          "kernel_ms": dom_ms, "kernel_bytes": dom_bytes},
-            "step_hbm": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes * steps_per_s / 1e9,
+            "step_hbm": {"algorithmic_bytes": sbytes, "achieved_gbs": sbytes * steps_per_s / 1e9,
+                         "frac": sbytes * steps_per_s / (peak * 1e9),
                          "model_bytes_216C": step_bytes_model(n),
                          "frac_of_model_roofline": step_bytes_model(n) * steps_per_s / (peak * 1e9)},
             "kernel_ms": {dns_b200.PASS_NAMES[p]: [float(kms[s, p]) for s in range(4)] for p in range(K)},
@@ -508,6 +595,8 @@ def main() -> int:
             "gpu_launches": dns_b200.KERNELS_PER_STEP * args.steps,
             "mixed": mixed,
             "ensemble": ens,
+            "n512": big,
+            "adjoint": adj,
             "clocks": clk,
             "cpu_baseline": cpu,
         }

@@ -395,6 +395,19 @@ def adjoint_energy(U, V, W, nu: float, dt: float, nsteps: int, snapshots: int = 
     return J.value, tuple(a.reshape(U.shape) for a in g), gnu.value
 
 
+def final_energy(U, V, W, nu: float, dt: float, nsteps: int) -> float:
+    """J = E(T) of adjoint_energy without its gradient: the forward sweep of
+    dns_adjoint_energy alone (all gradient pointers NULL), same arithmetic,
+    so J is the value adjoint_energy returns."""
+    lib = load_library()
+    U, V, W = _f64(U), _f64(V), _f64(W)
+    n = round(U.size ** (1.0 / 3))
+    J = ctypes.c_double()
+    _check(lib.dns_adjoint_energy(n, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, 1,
+                                  ctypes.byref(J), None, None, None, None))
+    return J.value
+
+
 def scale_diagnostics(eh, el, oh, ol, n):
     """main.c:265-266: long double sums times (double) invn3 * invn3."""
     invn3 = 1.0 / (n * n * n)

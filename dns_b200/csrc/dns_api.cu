@@ -235,6 +235,12 @@ struct Ops {
     return cudaSuccess;
   }
 
+  template <int KIND>
+  static void zpass(const Group &G, cudaStream_t st, C *work, R *stale, R invn3) {
+    k_zstage<R, N, KIND><<<zsgrid<KIND>(G.nruns), ZC<R, N, KIND>::THREADS, ZS_SMEM<KIND>, st>>>(
+        work, stale, tw(G), G.g, invn3);
+  }
+
   static C *slot(const Group &G, int s) { return (C *)G.S + (long long)s * G.g.slot; }
   static const C *tw(const Group &G) { return (const C *)G.tw; }
 
@@ -274,11 +280,11 @@ struct Ops {
         break;
       case 2:
         if (s == 0)
-          k_zstage<R, N, 0><<<zsgrid<0>(G.nruns), ZC<R, N, 0>::THREADS, ZS_SMEM<0>, st>>>(work, stale, tw(G), g, invn3);
+          zpass<0>(G, st, work, stale, invn3);
         else if (s < 3)
-          k_zstage<R, N, 1><<<zsgrid<1>(G.nruns), ZC<R, N, 1>::THREADS, ZS_SMEM<1>, st>>>(work, stale, tw(G), g, invn3);
+          zpass<1>(G, st, work, stale, invn3);
         else
-          k_zstage<R, N, 2><<<zsgrid<2>(G.nruns), ZC<R, N, 2>::THREADS, ZS_SMEM<2>, st>>>(work, stale, tw(G), g, invn3);
+          zpass<2>(G, st, work, stale, invn3);
         break;
       case 3:
       case 4: {
@@ -1323,6 +1329,14 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
     cudaError_t e = cudaMemcpyAsync(&d, A.G.diag_out, sizeof(double4), cudaMemcpyDeviceToHost, A.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  }
+  // J alone: the forward sweep is all it takes (no snapshots are needed
+  // beyond the first, and no reverse sweep runs)
+  const bool want_grad = gU || gV || gW || gnu;
+  if (r == DNS_OK && !want_grad) {
+    if (J) *J = (d.x + d.y) * (invn3 * invn3);
+    cleanup();
+    return r;
   }
   if (r == DNS_OK) {
     // lambda(T) = dE/dU_hat = 2 invn3^2 U_hat(T); the stale velocity at T

@@ -456,13 +456,59 @@ __device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N, KIND>::E], int t, FAB fa
   }
 }
 
+// The forward half of the z pass for one line: (N_x, N_y) as one complex
+// FFT, then N_z (main.c:378-380); only kz <= kcut is stored (N enters the
+// update through the 2/3 rule only).  `row` = the line's row of work slot 0.
+template <class R, int N, int KIND, class Idx, class Sync>
+__device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
+                                               const R (&nx)[ZC<R, N, KIND>::E],
+                                               const R (&ny)[ZC<R, N, KIND>::E],
+                                               const R (&nz)[ZC<R, N, KIND>::E], int t,
+                                               const cx<R> *tw, cx<R> *xb, Idx idx, Sync sync,
+                                               cx<R> *row, const Geo &g, bool ok) {
+  using C = cx<R>;
+  using Z = ZC<R, N, KIND>;
+  constexpr int E = Z::E, T = Z::T, M = Z::M;
+  const int KZ = g.kcut < M ? g.kcut : M;
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
+  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
+#pragma unroll
+  for (int e = 0; e < E; e++) xb[idx(t + T * e)] = y[e];
+  sync();
+  C *oU = row + SU * g.slot, *oV = row + SV * g.slot;
+#pragma unroll
+  for (int e = 0; e <= E / 2; e++) {
+    const int k = t + T * e;
+    if (k <= KZ) {
+      const C z = y[e], p = xb[idx((N - k) & (N - 1))];
+      const C a = cmk<C>(R(0.5) * (z.x + p.x), R(0.5) * (z.y - p.y));  // (Z + conj P) / 2
+      const C d = cmk<C>(R(0.5) * (z.x - p.x), R(0.5) * (z.y + p.y));  // (Z - conj P) / 2
+      if (ok) {
+        oU[k] = a;
+        oV[k] = cmk<C>(d.y, -d.x);  // -i d
+      }
+    }
+  }
+  sync();
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nz[e], R(0));
+  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
+  C *oW = row + SW * g.slot;
+#pragma unroll
+  for (int e = 0; e <= E / 2; e++) {
+    const int k = t + T * e;
+    if (k <= KZ && ok) oW[k] = y[e];
+  }
+}
+
 template <class R, int N, int KIND>
 __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     k_zstage(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg, Geo g,
              R invn3) {
   using C = cx<R>;
   using Z = ZC<R, N, KIND>;
-  constexpr int E = Z::E, T = Z::T, M = Z::M;
+  constexpr int E = Z::E, T = Z::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = (C *)smem_raw;  // stage twiddles of the z plan (<= N entries)
   build_stage_tw<N, typename Z::P>(tw, twg, N);
@@ -694,39 +740,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
       }
     }
   }
-  // forward: (N_x, N_y) as one complex FFT, then N_z  (main.c:378-380);
-  // only kz <= kcut is stored: N enters the update through the 2/3 rule only
-  const int KZ = g.kcut < M ? g.kcut : M;
-#pragma unroll
-  for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
-  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
-#pragma unroll
-  for (int e = 0; e < E; e++) xb[idx(t + T * e)] = y[e];
-  sync();
-  C *oU = work + SU * g.slot + off, *oV = work + SV * g.slot + off;
-#pragma unroll
-  for (int e = 0; e <= E / 2; e++) {
-    const int k = t + T * e;
-    if (k <= KZ) {
-      const C z = y[e], p = xb[idx((N - k) & (N - 1))];
-      const C a = cmk<C>(R(0.5) * (z.x + p.x), R(0.5) * (z.y - p.y));  // (Z + conj P) / 2
-      const C d = cmk<C>(R(0.5) * (z.x - p.x), R(0.5) * (z.y + p.y));  // (Z - conj P) / 2
-      if (ok) {
-        oU[k] = a;
-        oV[k] = cmk<C>(d.y, -d.x);  // -i d
-      }
-    }
-  }
-  sync();
-#pragma unroll
-  for (int e = 0; e < E; e++) y[e] = cmk<C>(nz[e], R(0));
-  line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
-  C *oW = work + SW * g.slot + off;
-#pragma unroll
-  for (int e = 0; e <= E / 2; e++) {
-    const int k = t + T * e;
-    if (k <= KZ && ok) oW[k] = y[e];
-  }
+  zstage_forward<R, N, KIND>(y, nx, ny, nz, t, tw, xb, idx, sync, work + off, g, ok);
 }
 
 // ---------------------------------------------------------------------------
@@ -738,8 +752,9 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
 //   ST 0:   next = u0 + b0 dU,  acc = u0 + a0 dU      (u_s == u0)
 //   ST 1,2: next = u0 + b dU,   acc += a dU
 //   ST 3:   u0   = acc + a3 dU   (the state of the next step)
-// A pure streaming kernel, one thread per half-spectrum point.  The
-// arithmetic is FP64 for both storage types (the FP32 path rounds on store).
+// A pure streaming kernel, one thread per half-spectrum point (two in FP32).
+// The FP64 path computes in FP64; the mixed path computes in FP32 with the
+// viscous coefficient nu dt |k|^2 formed in FP64 (update_point_f32).
 // ---------------------------------------------------------------------------
 // pointers are those of run 0; run r adds r * run_spec.  coef[2 r] = nu,
 // coef[2 r + 1] = dt of run r (device memory, so a captured graph picks up
@@ -820,6 +835,53 @@ __device__ __forceinline__ void update_point(const UpdIn<R> &in, UpdOut<R> &out,
   }
 }
 
+// The mixed path's update: FP32 arithmetic for the projection and the RK
+// axpys (the storage precision), FP64 only for the viscous coefficient
+// nu dt |k|^2, which is formed in FP64 and rounded once.  |k|^2 and the
+// wavenumbers are integers below 2^24, exact in FP32; dt and the RK
+// coefficients are rounded once per launch (rk = (dt, a, b) as floats).
+template <int ST>
+__device__ __forceinline__ void update_point_f32(const UpdIn<float> &in, UpdOut<float> &out,
+                                                 const Geo &g, float dtf, double nudt, float ra,
+                                                 float rb, int i, int j, int col) {
+  const int ikx = kwave(i, g.n), iky = kwave(j, g.n);
+  const float kx = (float)ikx, ky = (float)iky, kz = (float)col;
+  const bool inm = (ikx < 0 ? -ikx : ikx) <= g.kcut && (iky < 0 ? -iky : iky) <= g.kcut &&
+                   col <= g.kcut;
+  const float2 zero = make_float2(0.f, 0.f);
+  float2 du = inm ? cscale(in.n[0], dtf) : zero;
+  float2 dv = inm ? cscale(in.n[1], dtf) : zero;
+  float2 dw = inm ? cscale(in.n[2], dtf) : zero;
+  const int ikk = ikx * ikx + iky * iky + col * col;
+  const float kk = (float)ikk;
+  float2 P;
+  if (ikk > 0) {
+    P.x = __fdiv_rn(du.x * kx + dv.x * ky + dw.x * kz, kk);
+    P.y = __fdiv_rn(du.y * kx + dv.y * ky + dw.y * kz, kk);
+  } else {
+    P = zero;
+  }
+  const float c = (float)(nudt * (double)ikk);
+  du = make_float2(du.x - (P.x * kx + c * in.us[0].x), du.y - (P.y * kx + c * in.us[0].y));
+  dv = make_float2(dv.x - (P.x * ky + c * in.us[1].x), dv.y - (P.y * ky + c * in.us[1].y));
+  dw = make_float2(dw.x - (P.x * kz + c * in.us[2].x), dw.y - (P.y * kz + c * in.us[2].y));
+  out.p = P;
+  auto axpy = [](float2 x, float s, float2 y) { return make_float2(x.x + s * y.x, x.y + s * y.y); };
+  const float2 d[3] = {du, dv, dw};
+#pragma unroll
+  for (int f = 0; f < 3; f++) {
+    if (ST == 0) {  // us == u0
+      out.o1[f] = axpy(in.us[f], rb, d[f]);
+      out.o2[f] = axpy(in.us[f], ra, d[f]);
+    } else if (ST < 3) {
+      out.o1[f] = axpy(in.z[f], rb, d[f]);
+      out.o2[f] = axpy(in.a[f], ra, d[f]);
+    } else {
+      out.o1[f] = axpy(in.a[f], ra, d[f]);
+    }
+  }
+}
+
 constexpr int UPD_THREADS = 128;
 // adjacent points per vector access: two float2 make one 16-byte access
 template <class R>
@@ -888,7 +950,11 @@ __global__ void __launch_bounds__(UPD_THREADS)
         if (ST == 1 || ST == 2) in.z[f] = VT::get(lz[f], v);
         if (ST != 0) in.a[f] = VT::get(la[f], v);
       }
-      update_point<R, ST>(in, res[v], g, sa, nu, dt, (int)(row / N), (int)(row % N), col0 + v);
+      if constexpr (sizeof(R) == 4)
+        update_point_f32<ST>(in, res[v], g, (float)dt, nu * dt, (float)sa.a, (float)sa.b,
+                             (int)(row / N), (int)(row % N), col0 + v);
+      else
+        update_point<R, ST>(in, res[v], g, sa, nu, dt, (int)(row / N), (int)(row % N), col0 + v);
     }
   }
   V *o1 = (V *)(ST == 3 ? sa.u0 : sa.next), *o2 = (V *)sa.acc, *vp = (V *)sa.ph;

@@ -189,7 +189,8 @@ int dns_ens_synchronize(dns_ens *e);
  * nu (gnu).  FP64.  The transposed step is hand-written; forward states are
  * recomputed from `snapshots` stored step states (>= 1, the initial state
  * included) placed by a binomial split of the step range, so memory is
- * independent of nsteps.  Any output pointer may be NULL. */
+ * independent of nsteps.  Any output pointer may be NULL; with all four
+ * gradient pointers NULL only the forward sweep runs (J alone). */
 int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
                        double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
                        double *gW, double *gnu);

@@ -74,7 +74,9 @@ def test_adjoint_torch_autograd(dns):
     nut = torch.tensor(nu, dtype=torch.float64, requires_grad=True)
     J = FinalEnergy.apply(u0, nut, dt, nsteps, 3)
     (3.0 * J).backward()
-    _, g, gnu = dns.adjoint_energy(*u0.detach().numpy(), nu, dt, nsteps, 3)
+    Ja, g, gnu = dns.adjoint_energy(*u0.detach().numpy(), nu, dt, nsteps, 3)
+    # the forward call ran the forward sweep alone, with the same arithmetic
+    assert J.item() == Ja == dns.final_energy(*u0.detach().numpy(), nu, dt, nsteps)
     assert np.allclose(u0.grad.numpy(), 3.0 * np.stack(g), rtol=0, atol=0)
     assert nut.grad.item() == 3.0 * gnu
 
