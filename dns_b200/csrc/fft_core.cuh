@@ -196,11 +196,13 @@ struct StageTw {
 };
 
 // Fill the stage tables of plan P for a line of length L from the length-n
-// table twg[k] = exp(-2 pi i k / n) (global memory).  Caller syncs.
+// table twg[k] = exp(-2 pi i k / n) (global memory), threads tid of
+// nthreads.  Caller syncs.
 template <int L, class P, class C>
-__device__ __forceinline__ void build_stage_tw(C *st, const C *__restrict__ twg, int n) {
+__device__ __forceinline__ void build_stage_tw(C *st, const C *__restrict__ twg, int n, int tid,
+                                               int nthreads) {
   using S = StageTw<P>;
-  for (int i = threadIdx.x; i < S::SIZE; i += blockDim.x) {
+  for (int i = tid; i < S::SIZE; i += nthreads) {
     int nsv, R, loc;
     if (i < S::O2) {
       nsv = S::N1; R = P::R1; loc = i - S::O1;

@@ -91,6 +91,25 @@ struct ColIdx {
 struct BlockSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
+// barrier of a sub-block of `count` threads (a multiple of 32) with its own
+// hardware barrier id (1..15): several work items share one block of the
+// persistent ensemble kernel
+struct NamedSync {
+  int id, count;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+  }
+};
+// coordinates of one work item: the launch's blockIdx / threadIdx in the
+// standalone kernels, a virtual block of the persistent ensemble kernel
+struct Blk {
+  int x, y, z;  // block index
+  int tid;      // thread index within the item
+  int nt;       // threads of the item
+};
+__device__ __forceinline__ Blk launch_blk() {
+  return Blk{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)threadIdx.x, (int)blockDim.x};
+}
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
@@ -99,10 +118,13 @@ template <int SH>
 struct PadShift {
   __device__ __forceinline__ int operator()(int pos) const { return pos + (pos >> SH); }
 };
-template <bool BLOCK>
+// exchange barrier of one line: the block's barrier when a line spans
+// several warps, else the warp's
+template <bool BLOCK, class BSync = BlockSync>
 struct LineSync {
+  BSync bsync{};
   __device__ __forceinline__ void operator()() const {
-    if (BLOCK) __syncthreads(); else __syncwarp();
+    if (BLOCK) bsync(); else __syncwarp();
   }
 };
 
@@ -111,27 +133,27 @@ struct LineSync {
 // grid: (nfp / W, n, njobs * nruns); block: (N / E) * W threads
 // (W = ColW<R, AXIS, N>::W).
 // ---------------------------------------------------------------------------
-template <class R, int N, int AXIS, bool FWD>
+template <class R, int N, int AXIS, bool FWD, class Sync>
 __device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
                                              const cx<R> *__restrict__ twg, const Geo &g,
-                                             const ColJobs &jobs) {
+                                             const ColJobs &jobs, const Blk b, Sync sync,
+                                             unsigned char *smem) {
   using C = cx<R>;
   constexpr int W = ColW<R, AXIS, N>::W;
   constexpr int E = Plan<N>::E, T = N / E;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *st = (C *)smem_raw;  // stage twiddles (<= N entries)
+  C *st = (C *)smem;  // stage twiddles (<= N entries)
   C *xb = st + N;
-  build_stage_tw<N, Plan<N>>(st, twg, N);
-  __syncthreads();
-  const int p = threadIdx.x % W, t = threadIdx.x / W;
-  const int col = blockIdx.x * W + p;
+  build_stage_tw<N, Plan<N>>(st, twg, N, b.tid, b.nt);
+  sync();
+  const int p = b.tid % W, t = b.tid / W;
+  const int col = b.x * W + p;
   const bool ok = col < g.nf;
   // j for the x pass, i for the y pass; a masked x pass is launched on the
   // 2 kcut + 1 rows with |ky| <= kcut only: rows past kcut map to n - kcut..
-  int fixed = blockIdx.y;
+  int fixed = b.y;
   if (AXIS == 0 && jobs.masked && fixed > g.kcut) fixed += N - (2 * g.kcut + 1);
-  const int job = blockIdx.z % jobs.njobs;
-  const long long rb = (long long)(blockIdx.z / jobs.njobs) * g.run_spec;
+  const int job = b.z % jobs.njobs;
+  const long long rb = (long long)(b.z / jobs.njobs) * g.run_spec;
   in += rb;
   out += rb;
   long long base, rs;
@@ -169,7 +191,7 @@ __device__ __forceinline__ void colpass_body(const cx<R> *__restrict__ in, cx<R>
         v[e] = cmk<C>(a.x + k * v[e].y, a.y - k * v[e].x);  // add - i k f
       }
     }
-    line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, BlockSync{});
+    line_fft<N, Plan<N>, FWD>(v, t, st, xb, ColIdx<W>{p}, sync);
     if (ok) {
       C *dst = out + (long long)dst_slot * g.slot + base;
 #pragma unroll
@@ -185,7 +207,8 @@ template <class R, int N, int AXIS, bool FWD>
 __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
     k_colpass(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
               const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
-  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs, launch_blk(), BlockSync{}, smem_raw);
 }
 
 // The same pass with its registers held so that MINB blocks fit per SM: the
@@ -197,7 +220,8 @@ template <class R, int N, int AXIS, bool FWD, int MINB>
 __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W, MINB)
     k_colpass_minb(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
                    const cx<R> *__restrict__ twg, Geo g, ColJobs jobs) {
-  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs, launch_blk(), BlockSync{}, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -291,7 +315,7 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
   C *tw = (C *)smem_raw;  // full table exp(-2 pi i k / N): pre/post twiddles
   C *st = tw + N;         // stage twiddles of ZPlan<N/2>
   for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
-  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
   const int lane0 = (threadIdx.x & 31) - t;
@@ -327,7 +351,7 @@ __global__ void __launch_bounds__(ZCfg<N>::THREADS)
   C *tw = (C *)smem_raw;
   C *st = tw + N;
   for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = twg[k];
-  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N);
+  build_stage_tw<N / 2, ZPlan<N / 2>>(st, twg, N, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lid = threadIdx.x / TZ, t = threadIdx.x % TZ;
   const int lane0 = (threadIdx.x & 31) - t;
@@ -387,7 +411,9 @@ struct ZC {
   static constexpr int WANT = S2 ? 64 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
-  static constexpr int MINB = S2 ? 4 : 3;         // blocks per SM (register cap 255 / 170)
+  // blocks per SM: register cap 255 (FP64), 128 (FP32 first stage, which
+  // keeps no velocity in registers), 170 (other FP32 stages)
+  static constexpr int MINB = S2 ? 4 : (F32 && KIND == 0) ? 4 : 3;
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
   // staged scalars per line: S2 none (first stage), two (middle stage) or
@@ -502,26 +528,28 @@ __device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
   }
 }
 
-template <class R, int N, int KIND>
-__global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
-    k_zstage(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg, Geo g,
-             R invn3) {
+// One block of the z pass: Z::LINES lines starting at line b.x * LINES of
+// run b.y (block-wide barriers through `bsync`, which lines of more than 32
+// threads also use between FFT stages).
+template <class R, int N, int KIND, class BSync>
+__device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restrict__ stale,
+                                            const cx<R> *__restrict__ twg, const Geo &g, R invn3,
+                                            const Blk b, BSync bsync, unsigned char *smem) {
   using C = cx<R>;
   using Z = ZC<R, N, KIND>;
   constexpr int E = Z::E, T = Z::T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *tw = (C *)smem_raw;  // stage twiddles of the z plan (<= N entries)
-  build_stage_tw<N, typename Z::P>(tw, twg, N);
-  __syncthreads();
-  const int lid = threadIdx.x / T, t = threadIdx.x % T;
+  C *tw = (C *)smem;  // stage twiddles of the z plan (<= N entries)
+  build_stage_tw<N, typename Z::P>(tw, twg, N, b.tid, b.nt);
+  bsync();
+  const int lid = b.tid / T, t = b.tid % T;
   C *xb = tw + N + lid * Z::XB;
   R *st = (R *)(tw + N + Z::LINES * Z::XB) + lid * Z::STASH;
   // own points of staged field f: st[(f * E + e) * T + t]
   auto SU_ = [&](int f, int e) -> R & { return st[(f * E + e) * T + t]; };
-  const long long line = (long long)blockIdx.x * Z::LINES + lid;
+  const long long line = (long long)b.x * Z::LINES + lid;
   const bool ok = line < (long long)N * N;
-  work += (long long)blockIdx.y * g.run_spec;  // run of the batch
-  stale += (long long)blockIdx.y * g.run_real;
+  work += (long long)b.y * g.run_spec;  // run of the batch
+  stale += (long long)b.y * g.run_real;
   const long long off = line * g.nfp;
   const C *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
   const C *pW = work + SW * g.slot + off, *pOMZ = work + SOMZ * g.slot + off;
@@ -540,7 +568,7 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
     return ld(pOMZ, s);
   };
   auto f_zero = [&](int) -> C { return czero<C>(); };
-  const LineSync<(T > 32)> sync{};
+  const LineSync<(T > 32), BSync> sync{bsync};
   const PadShift<Z::PADSH> idx{};
   const long long roff = line * N;
 
@@ -743,6 +771,14 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
   zstage_forward<R, N, KIND>(y, nx, ny, nz, t, tw, xb, idx, sync, work + off, g, ok);
 }
 
+template <class R, int N, int KIND>
+__global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
+    k_zstage(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg, Geo g,
+             R invn3) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  zstage_body<R, N, KIND>(work, stale, twg, g, invn3, launch_blk(), BlockSync{}, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // E2: after the x forward transform of the three N slots (E1), the pointwise
 // update of main.c:381-413 on the full half spectrum:
@@ -906,9 +942,10 @@ struct UpdVec<float> {
 // grid: (ceil(n^2 nfp / VP / UPD_THREADS), nruns).  Thread = VP adjacent
 // points of the padded slot (padding columns included and skipped), so that
 // the row, kx and ky of a point come from divisions by compile-time constants.
+// One chunk of UPD_THREADS threads: chunk b.x of run b.y.
 template <class R, int N, int ST>
-__global__ void __launch_bounds__(UPD_THREADS)
-    k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
+__device__ __forceinline__ void update_body(const cx<R> *__restrict__ nl, const Geo &g,
+                                            const StageArgs<R> &sa, const Blk b) {
   using VT = UpdVec<R>;
   using V = typename VT::T;
   constexpr int VP = VT::VP;
@@ -916,13 +953,13 @@ __global__ void __launch_bounds__(UPD_THREADS)
   constexpr int NFP = (NF + PitchW<R>::W - 1) / PitchW<R>::W * PitchW<R>::W;
   constexpr unsigned NPAD = (unsigned)N * N * NFP;
   static_assert(NFP % VP == 0, "vector access must not straddle rows");
-  const unsigned q0 = (blockIdx.x * (unsigned)UPD_THREADS + threadIdx.x) * VP;
+  const unsigned q0 = ((unsigned)b.x * (unsigned)UPD_THREADS + (unsigned)b.tid) * VP;
   if (q0 >= NPAD) return;
   const unsigned row = q0 / NFP;
   const int col0 = (int)(q0 - row * NFP);
   if (col0 >= NF) return;
-  const long long rb = (long long)blockIdx.y * g.run_spec;
-  const double nu = sa.coef[2 * blockIdx.y], dt = sa.coef[2 * blockIdx.y + 1];
+  const long long rb = (long long)b.y * g.run_spec;
+  const double nu = sa.coef[2 * b.y], dt = sa.coef[2 * b.y + 1];
   const long long vo = (rb + q0) / VP, vs = g.slot / VP;  // vector index, slot stride
   const V *vn = (const V *)nl, *vus = (const V *)sa.us, *vz = (const V *)sa.u0,
           *va = (const V *)sa.acc;
@@ -985,6 +1022,12 @@ __global__ void __launch_bounds__(UPD_THREADS)
     }
     if (sa.ph) sa.ph[o] = res[0].p;
   }
+}
+
+template <class R, int N, int ST>
+__global__ void __launch_bounds__(UPD_THREADS)
+    k_update(const cx<R> *__restrict__ nl, Geo g, StageArgs<R> sa) {
+  update_body<R, N, ST>(nl, g, sa, launch_blk());
 }
 
 // ---------------------------------------------------------------------------
