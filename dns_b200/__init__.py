@@ -72,6 +72,7 @@ _SIGS = {
     "dns_set_stale": (ctypes.c_int, [_P, _P]),
     "dns_get_info": (ctypes.c_int, [_P, ctypes.POINTER(_Info)]),
     "dns_get_stream": (_P, [_P]),
+    "dns_get_schedule": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_long]),
     "dns_synchronize": (ctypes.c_int, [_P]),
     "dns_time_kernels": (ctypes.c_int, [_P, _D, _D, ctypes.c_long, ctypes.POINTER(_D)]),
     "dns_diagnostics_noalloc": (ctypes.c_int, [ctypes.c_long, _P, _P, _P]),
@@ -232,6 +233,12 @@ class Context:
         i = _Info()
         _check(self._lib.dns_get_info(self._h, ctypes.byref(i)))
         return {f: getattr(i, f) for f, _ in _Info._fields_}
+
+    def schedule(self) -> str:
+        """The autotuner's kernel schedule for this grid size (dns_get_schedule)."""
+        buf = ctypes.create_string_buffer(4096)
+        _check(self._lib.dns_get_schedule(self._h, buf, len(buf)))
+        return buf.value.decode()
 
     def time_kernels(self, nu: float, dt: float, nsteps: int) -> np.ndarray:
         ms = (ctypes.c_double * KERNELS_PER_STEP)()

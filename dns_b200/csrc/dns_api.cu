@@ -24,6 +24,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -207,32 +208,142 @@ struct Ops {
   template <int KIND>
   static constexpr size_t ZS_SMEM = ZC<R, N, KIND>::SMEM;
 
-  // the column-pass kernel of this precision and size: FP32 n = 256 tiles run
-  // the variant held to 4 blocks per SM
-  template <int AXIS, bool FWD>
-  static auto colkern() {
-    if constexpr (sizeof(R) == 4 && N == 256)
-      return k_colpass_minb<R, N, AXIS, FWD, 4>;
-    else
+  // Column-pass register schedules.  Candidate I of a pass is the same
+  // kernel compiled with a minimum of ColCands::m[I] resident blocks per SM
+  // (0: the compiler's own register choice); the candidates differ only in
+  // register allocation, so every one computes bit-identical results.  The
+  // autotuner (tune()) times them once per process and size and keeps the
+  // fastest; sizes below 64 have the compiler's choice only.
+  using ColFn = void (*)(const C *, C *, const C *, Geo, ColJobs);
+  template <int AXIS>
+  using Cands = ColCands<(N >= 64 ? CT<AXIS> : 0), (int)sizeof(C)>;
+  template <int AXIS, bool FWD, int I>
+  static ColFn col_cand() {
+    constexpr int m = Cands<AXIS>::m[I];
+    if constexpr (m == 0)
       return k_colpass<R, N, AXIS, FWD>;
+    else
+      return k_colpass_minb<R, N, AXIS, FWD, m>;
+  }
+  template <int AXIS, bool FWD, int I = 0>
+  static ColFn col_cand_at(int i) {
+    if constexpr (I + 1 < Cands<AXIS>::n) {
+      if (i != I) return col_cand_at<AXIS, FWD, I + 1>(i);
+    }
+    return col_cand<AXIS, FWD, I>();
+  }
+  // chosen candidate of [AXIS][FWD] and its measured time per launch (ms)
+  static inline int col_pick[2][2] = {{0, 0}, {0, 0}};
+  static inline float col_ms[2][2][8] = {};
+  static inline bool tuned = false;
+  template <int AXIS, bool FWD>
+  static ColFn colkern() {
+    return col_cand_at<AXIS, FWD>(col_pick[AXIS][FWD]);
   }
 
   template <class K>
   static cudaError_t allow(K kern, size_t smem) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
+  template <int AXIS, bool FWD>
+  static cudaError_t allow_cands() {
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < Cands<AXIS>::n && e == cudaSuccess; i++)
+      e = allow(col_cand_at<AXIS, FWD>(i), COL_SMEM<AXIS>);
+    return e;
+  }
   static cudaError_t setup() {
     cudaError_t e;
-    if ((e = allow(colkern<0, false>(), COL_SMEM<0>))) return e;
-    if ((e = allow(colkern<0, true>(), COL_SMEM<0>))) return e;
-    if ((e = allow(colkern<1, false>(), COL_SMEM<1>))) return e;
-    if ((e = allow(colkern<1, true>(), COL_SMEM<1>))) return e;
+    if ((e = allow_cands<0, false>())) return e;
+    if ((e = allow_cands<0, true>())) return e;
+    if ((e = allow_cands<1, false>())) return e;
+    if ((e = allow_cands<1, true>())) return e;
     if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM<0>))) return e;
     if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM<1>))) return e;
     if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM<2>))) return e;
     if ((e = allow(k_zr2c<R, N>, Z_SMEM))) return e;
     if ((e = allow(k_zc2r<R, N>, Z_SMEM))) return e;
     return cudaSuccess;
+  }
+
+  // ---- autotuner of the column-pass register schedules ----
+  template <int AXIS, bool FWD>
+  static cudaError_t time_cands(const Group &G1, cudaStream_t st, const ColJobs &jobs,
+                                cudaEvent_t e0, cudaEvent_t e1, int force) {
+    constexpr int n = Cands<AXIS>::n;
+    int best = 0;
+    for (int i = 0; i < n; i++) {
+      col_pick[AXIS][FWD] = i;
+      colpass_io<AXIS, FWD>(G1, st, (C *)G1.S, (C *)G1.S, jobs, 1);  // warm-up
+      cudaError_t e = cudaEventRecord(e0, st);
+      for (int r = 0; r < 3 && e == cudaSuccess; r++) {
+        colpass_io<AXIS, FWD>(G1, st, (C *)G1.S, (C *)G1.S, jobs, 1);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) return e;
+      col_ms[AXIS][FWD][i] = ms / 3.f;
+      if (col_ms[AXIS][FWD][i] < col_ms[AXIS][FWD][best]) best = i;
+    }
+    col_pick[AXIS][FWD] = force >= 0 ? (force < n ? force : n - 1) : best;
+    return cudaSuccess;
+  }
+  // Time every register schedule of the four column passes of an RK stage
+  // (their real job tables, on the work slots of run 0, whose contents do
+  // not matter to an FFT's timing) and keep the fastest of each; once per
+  // process and size.  DNS_B200_TUNE=0 keeps the compiler's schedule,
+  // DNS_B200_TUNE=f<k> forces candidate k (the last where there are fewer).
+  static cudaError_t tune(const Group &G, cudaStream_t st, bool *ran) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    *ran = false;
+    if (tuned) return cudaSuccess;
+    const char *env = getenv("DNS_B200_TUNE");
+    if (env && strcmp(env, "0") == 0) {
+      tuned = true;
+      return cudaSuccess;
+    }
+    const int force = (env && env[0] == 'f') ? atoi(env + 1) : -1;
+    const Group G1 = G.one(0);
+    const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+    ColJobs jm = jobs_map(io, io, 3);
+    jm.masked = 1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = time_cands<0, false>(G1, st, jobs_pass_a(SLOT_WORK), e0, e1, force);
+    if (e == cudaSuccess) e = time_cands<1, false>(G1, st, jobs_pass_b(false), e0, e1, force);
+    if (e == cudaSuccess) e = time_cands<1, true>(G1, st, jm, e0, e1, force);
+    if (e == cudaSuccess) e = time_cands<0, true>(G1, st, jm, e0, e1, force);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e == cudaSuccess) tuned = true;
+    *ran = true;
+    return e;
+  }
+  // text description of the chosen schedules
+  static std::string schedule() {
+    std::string out;
+    const char *name[2][2] = {{"x inverse", "x forward"}, {"y inverse", "y forward"}};
+    char buf[160];
+    for (int a = 0; a < 2; a++)
+      for (int f = 0; f < 2; f++) {
+        const int n = a == 0 ? Cands<0>::n : Cands<1>::n;
+        const int *m = a == 0 ? Cands<0>::m : Cands<1>::m;
+        const int k = col_pick[a][f];
+        snprintf(buf, sizeof buf, "%scolumn pass %s: min blocks/SM %d of {", out.empty() ? "" : "; ",
+                 name[a][f], m[k]);
+        out += buf;
+        for (int i = 0; i < n; i++) {
+          snprintf(buf, sizeof buf, "%s%d: %.4f ms", i ? ", " : "", m[i], col_ms[a][f][i]);
+          out += buf;
+        }
+        out += "}";
+      }
+    return out;
   }
 
   template <int KIND>
@@ -505,6 +616,14 @@ int group_init(Group &G, long n, int precision, unsigned flags, int nruns, cudaS
   CK(cudaMemsetAsync(G.S, 0, spec_b, st));
   CK(cudaMemsetAsync(G.stale, 0, stale_b, st));
   CK(cudaStreamSynchronize(st));
+  cudaError_t te = cudaSuccess;
+  bool ran = false;
+  dispatch(G, [&](auto ops) { te = decltype(ops)::tune(G, st, &ran); });
+  CK(te);
+  if (ran) {  // the tuner ran column passes on run 0's work slots: zero them again
+    CK(cudaMemsetAsync(G.slot_ptr(0, SLOT_WORK), 0, (size_t)7 * g.slot * G.csize, st));
+    CK(cudaStreamSynchronize(st));
+  }
   return DNS_OK;
 }
 
@@ -1013,6 +1132,14 @@ int dns_get_info(dns_ctx *c, dns_info_t *info) {
   info->device_bytes = c->grp.arena_bytes;
   info->slot_bytes = (size_t)c->grp.g.slot * c->grp.csize;
   info->kernels_per_step = c->kernels_per_step;
+  return DNS_OK;
+}
+
+int dns_get_schedule(dns_ctx *c, char *buf, long len) {
+  if (!c || !buf || len < 1) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  std::string s;
+  dispatch(c->grp, [&](auto ops) { s = decltype(ops)::schedule(); });
+  snprintf(buf, (size_t)len, "%s", s.c_str());
   return DNS_OK;
 }
 

@@ -211,11 +211,8 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W)
   colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs, launch_blk(), BlockSync{}, smem_raw);
 }
 
-// The same pass with its registers held so that MINB blocks fit per SM: the
-// FP32 tiles at n = 256 (256 threads) run 4 blocks at <= 64 registers (the
-// omega_z job's second tile would otherwise take 66, 3 blocks).  An explicit
-// ceiling is not applied to the other tiles: with one, the compiler trades
-// their occupancy for registers.
+// The same pass with its registers held so that MINB blocks fit per SM (a
+// register schedule the autotuner may pick).
 template <class R, int N, int AXIS, bool FWD, int MINB>
 __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W, MINB)
     k_colpass_minb(const cx<R> *__restrict__ in, cx<R> *__restrict__ out,
@@ -223,6 +220,46 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W, MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs, launch_blk(), BlockSync{}, smem_raw);
 }
+
+// Register-schedule candidates of a column-pass tile of THREADS threads with
+// complex values of CB bytes: minimum resident blocks per SM giving register
+// caps of about 255 (the compiler's choice, 0), 170, 128, 102, 85 and 64
+// (FP64 tiles stop at 80: at 64 they spill a kilobyte per thread).
+template <int THREADS, int CB>
+struct ColCands {
+  static constexpr int n = 1;
+  static constexpr int m[1] = {0};
+};
+template <>
+struct ColCands<64, 16> {
+  static constexpr int n = 5;
+  static constexpr int m[5] = {0, 6, 8, 10, 12};
+};
+template <>
+struct ColCands<128, 16> {
+  static constexpr int n = 5;
+  static constexpr int m[5] = {0, 3, 4, 5, 6};
+};
+template <>
+struct ColCands<256, 16> {
+  static constexpr int n = 3;
+  static constexpr int m[3] = {0, 2, 3};
+};
+template <>
+struct ColCands<128, 8> {
+  static constexpr int n = 6;
+  static constexpr int m[6] = {0, 3, 4, 5, 6, 8};
+};
+template <>
+struct ColCands<256, 8> {
+  static constexpr int n = 4;
+  static constexpr int m[4] = {0, 2, 3, 4};
+};
+template <>
+struct ColCands<512, 8> {
+  static constexpr int n = 3;
+  static constexpr int m[3] = {0, 1, 2};
+};
 
 // ---------------------------------------------------------------------------
 // Real transforms of single z lines (initial r2c, dump c2r) through a

@@ -136,6 +136,14 @@ typedef struct {
   int kernels_per_step;    /* kernel launches in one RK4 step */
 } dns_info_t;
 int dns_get_info(dns_ctx *ctx, dns_info_t *info);
+/* The kernel schedule the library's autotuner chose for this context's grid
+ * size and precision (no counterpart in the reference): for each column
+ * pass, the register schedule (minimum resident blocks per SM) picked by
+ * timing every compiled candidate once per process, with the measured
+ * times.  All candidates compute bit-identical results.  The environment
+ * variable DNS_B200_TUNE=0 keeps the compiler's schedule; DNS_B200_TUNE=f<k>
+ * forces candidate k.  Writes a NUL-terminated text of at most len bytes. */
+int dns_get_schedule(dns_ctx *ctx, char *buf, long len);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time work
  * with CUDA events on it. */
