@@ -402,6 +402,9 @@ def main() -> int:
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-n512", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
+                    help="profiling run: set-up and --warmup steps, then exactly one RK4 "
+                         "step between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -413,6 +416,18 @@ def main() -> int:
     import dns_b200
 
     torch.cuda.set_device(local)
+    if args.profile:
+        prec = dns_b200.DNS_PREC_FP64 if args.profile == "fp64" else dns_b200.DNS_PREC_MIXED
+        with dns_b200.Context(args.n, prec) as c:
+            c.set_tgv()
+            c.step(NU, DT, max(1, args.warmup))
+            c.synchronize()
+            torch.cuda.profiler.start()
+            c.step(NU, DT, 1)
+            c.synchronize()
+            torch.cuda.profiler.stop()
+            print(json.dumps({"profile": args.profile, "n": args.n, "schedule": c.schedule()}))
+        return 0
     pg = None
     if world > 1:
         import datetime

@@ -234,7 +234,7 @@ struct Ops {
   }
   // chosen candidate of [AXIS][FWD] and its measured time per launch (ms)
   static inline int col_pick[2][2] = {{0, 0}, {0, 0}};
-  static inline float col_ms[2][2][8] = {};
+  static inline float col_ms[2][2][16] = {};
   static inline bool tuned = false;
   template <int AXIS, bool FWD>
   static ColFn colkern() {
@@ -338,7 +338,7 @@ struct Ops {
                  name[a][f], m[k]);
         out += buf;
         for (int i = 0; i < n; i++) {
-          snprintf(buf, sizeof buf, "%s%d: %.4f ms", i ? ", " : "", m[i], col_ms[a][f][i]);
+          snprintf(buf, sizeof buf, "%s%d: %.4f ms", i ? ", " : "", m[i], (double)col_ms[a][f][i]);
           out += buf;
         }
         out += "}";

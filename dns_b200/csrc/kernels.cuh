@@ -221,10 +221,11 @@ __global__ void __launch_bounds__((N / Plan<N>::E) * ColW<R, AXIS, N>::W, MINB)
   colpass_body<R, N, AXIS, FWD>(in, out, twg, g, jobs, launch_blk(), BlockSync{}, smem_raw);
 }
 
-// Register-schedule candidates of a column-pass tile of THREADS threads with
-// complex values of CB bytes: minimum resident blocks per SM giving register
-// caps of about 255 (the compiler's choice, 0), 170, 128, 102, 85 and 64
-// (FP64 tiles stop at 80: at 64 they spill a kilobyte per thread).
+// Register-schedule candidates of a column-pass tile of THREADS threads
+// with complex values of CB bytes: a minimum of m[i] resident blocks per SM
+// (0: the compiler's register choice; otherwise register caps of about 170,
+// 128, 102, 85, 64; FP64 tiles stop at 80: at 64 they spill a kilobyte per
+// thread).
 template <int THREADS, int CB>
 struct ColCands {
   static constexpr int n = 1;

@@ -49,7 +49,7 @@ def test_every_schedule_is_bit_identical(dns_lib, tmp_path, n, prec, ncand):
 
 def test_tuned_schedule_is_the_fastest_timed(dns_lib, tmp_path):
     _, sched = _run(tmp_path, 256, 0, "1")
-    # "... min blocks/SM <m> of {<m0>: <t0> ms, <m1>: <t1> ms, ...}" per pass
+    # "column pass <name>: min blocks/SM <m> of {<m0>: <t0> ms, ...}" per pass
     for part in sched.split("; "):
         chosen = int(part.split("min blocks/SM ")[1].split(" ")[0])
         cands = part.split("{")[1].rstrip("}").split(", ")
