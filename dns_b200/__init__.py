@@ -29,6 +29,8 @@ DNS_ERR_STATE = 6
 DNS_PREC_FP64 = 0
 DNS_PREC_MIXED = 1
 DNS_FLAG_PRESSURE = 1
+DNS_FLAG_ENS_BATCHED = 2
+DNS_FLAG_ENS_PERSISTENT = 4
 
 SUPPORTED_N = (8, 16, 32, 64, 128, 256, 512)
 KERNELS_PER_STAGE = 6
@@ -89,6 +91,8 @@ _SIGS = {
     "dns_ens_get_spectral": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "dns_ens_get_stream": (_P, [_P]),
     "dns_ens_synchronize": (ctypes.c_int, [_P]),
+    "dns_ens_get_schedule": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_long]),
+    "dns_selftest_barrier_timeout": (ctypes.c_int, [_D, ctypes.POINTER(ctypes.c_int)]),
     "dns_adjoint_energy": (ctypes.c_int, [ctypes.c_long, _P, _P, _P, _D, _D, ctypes.c_long,
                                           ctypes.c_int, _P, _P, _P, _P, _P]),
 }
@@ -314,6 +318,12 @@ class Ensemble:
     def synchronize(self) -> None:
         _check(self._lib.dns_ens_synchronize(self._h))
 
+    def schedule(self) -> str:
+        """The schedule the ensemble runs and the timings that chose it."""
+        buf = ctypes.create_string_buffer(8192)
+        _check(self._lib.dns_ens_get_schedule(self._h, buf, len(buf)))
+        return buf.value.decode()
+
 
 _M64 = (1 << 64) - 1
 _GOLDEN64 = 0x9E3779B97F4A7C15
@@ -413,6 +423,16 @@ def final_energy(U, V, W, nu: float, dt: float, nsteps: int) -> float:
     _check(lib.dns_adjoint_energy(n, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, 1,
                                   ctypes.byref(J), None, None, None, None))
     return J.value
+
+
+def selftest_barrier_timeout(limit_s: float = 0.05) -> bool:
+    """Run the persistent kernel's barrier-wait self-test
+    (dns_selftest_barrier_timeout): True when a barrier wait that can never
+    complete gave up after limit_s and was reported."""
+    lib = load_library()
+    out = ctypes.c_int(0)
+    _check(lib.dns_selftest_barrier_timeout(limit_s, ctypes.byref(out)))
+    return bool(out.value)
 
 
 def scale_diagnostics(eh, el, oh, ol, n):

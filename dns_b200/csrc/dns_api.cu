@@ -19,12 +19,15 @@
 #include "adjoint.cuh"
 #include "init.cuh"
 #include "kernels.cuh"
+#include "persistent.cuh"
 
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -152,6 +155,15 @@ struct dns_ens {
   cudaGraphExec_t graph = nullptr;
   int nruns = 0;
   bool params_set = false;
+  // the persistent schedule: one cooperative launch per step
+  int mode = 0;                  // 0: batched launches, 1: persistent
+  void *pplan = nullptr;         // device PPlan<R>
+  PSync *psync = nullptr;        // device barrier state and error word
+  int pgrid = 0;                 // co-resident blocks
+  size_t psmem = 0;              // dynamic shared bytes per block
+  cudaGraphExec_t pgraph = nullptr;
+  bool pgraph_ok = false;        // the cooperative launch was captured
+  float step_ms[2] = {-1.f, -1.f};  // measured ms per step of each schedule
 };
 
 namespace {
@@ -216,7 +228,7 @@ struct Ops {
   // fastest; sizes below 64 have the compiler's choice only.
   using ColFn = void (*)(const C *, C *, const C *, Geo, ColJobs);
   template <int AXIS>
-  using Cands = ColCands<(N >= 64 ? CT<AXIS> : 0), (int)sizeof(C)>;
+  using Cands = ColCands<(N >= 64 ? (N / Plan<N>::E) * ColW<R, AXIS, N>::W : 0), (int)sizeof(C)>;
   template <int AXIS, bool FWD, int I>
   static ColFn col_cand() {
     constexpr int m = Cands<AXIS>::m[I];
@@ -376,61 +388,111 @@ struct Ops {
     return dim3((N * N + ZC<R, N, KIND>::LINES - 1) / ZC<R, N, KIND>::LINES, nruns);
   }
 
+  // Pass `k` (0..KERNELS_PER_STAGE-1) of RK stage `s` for all runs of G:
+  // what it runs, its job table or stage arguments, and its work items (the
+  // launch grid, threads and shared memory of one block).  The standalone
+  // launches (stage_kernel) and the persistent ensemble kernel's plan are
+  // both made from it.
+  static PPhase<R> describe(const Group &G, int s, int k) {
+    const Geo &g = G.g;
+    PPhase<R> P{};
+    P.gz = 1;
+    if (k == 0 || k == 1 || k == 3 || k == 4) {
+      P.kind = PK_COL;
+      P.axis = (k == 0 || k == 4) ? 0 : 1;
+      P.fwd = k >= 3;
+      if (k == 0) {
+        P.jobs = jobs_pass_a(s == 0 ? SLOT_SA : SLOT_SB);
+      } else if (k == 1) {
+        P.jobs = jobs_pass_b(s == 0);
+      } else {
+        // D: y forward, E1: x forward (in place on the three N slots); only
+        // the modes inside the 2/3 rule are computed and stored
+        const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+        P.jobs = jobs_map(io, io, 3);
+        P.jobs.masked = 1;
+      }
+      constexpr int cw0 = CW<0>, cw1 = CW<1>, ct0 = CT<0>, ct1 = CT<1>;
+      constexpr int sm0 = (int)COL_SMEM<0>, sm1 = (int)COL_SMEM<1>;
+      const int cw = P.axis == 0 ? cw0 : cw1;
+      // a masked pass covers the tiles holding kz <= kcut and, along x, the
+      // ky rows with |ky| <= kcut (kernels.cuh maps them back)
+      P.gx = P.jobs.masked ? g.kcut / cw + 1 : g.nfp / cw;
+      P.gy = (P.jobs.masked && P.axis == 0) ? 2 * g.kcut + 1 : N;
+      P.gz = P.jobs.njobs * G.nruns;
+      P.tpi = P.axis == 0 ? ct0 : ct1;
+      P.smem = P.axis == 0 ? sm0 : sm1;
+    } else if (k == 2) {
+      P.kind = PK_Z;
+      P.sub = s == 0 ? 0 : s < 3 ? 1 : 2;
+      const int lines = P.sub == 0 ? ZC<R, N, 0>::LINES : P.sub == 1 ? ZC<R, N, 1>::LINES
+                                                                      : ZC<R, N, 2>::LINES;
+      P.gx = (N * N + lines - 1) / lines;
+      P.gy = G.nruns;
+      P.tpi = ZC<R, N, 0>::THREADS;
+      P.smem = (int)(P.sub == 0 ? ZS_SMEM<0> : P.sub == 1 ? ZS_SMEM<1> : ZS_SMEM<2>);
+    } else {
+      P.kind = PK_UPD;
+      P.sub = s;
+      StageArgs<R> &sa = P.sa;
+      sa.u0 = slot(G, SLOT_SA);
+      sa.us = slot(G, s == 0 ? SLOT_SA : SLOT_SB);
+      sa.acc = slot(G, SLOT_ACC);
+      sa.next = slot(G, SLOT_SB);
+      sa.ph = (s == 3 && (G.flags & DNS_FLAG_PRESSURE)) ? slot(G, SLOT_P) : nullptr;
+      sa.coef = G.coef;
+      sa.a = RK_A[s];
+      sa.b = s < 3 ? RK_B[s] : 0.0;
+      const long long npad = (long long)N * N * g.nfp;
+      const int per = UPD_THREADS * UpdVec<R>::VP;
+      P.gx = (int)((npad + per - 1) / per);
+      P.gy = G.nruns;
+      P.tpi = UPD_THREADS;
+      P.smem = 0;
+    }
+    return P;
+  }
+
   // kernel `k` (0..KERNELS_PER_STAGE-1) of RK stage `s`, all runs of G
   static void stage_kernel(const Group &G, cudaStream_t st, int s, int k) {
     const Geo &g = G.g;
     C *work = slot(G, SLOT_WORK);
     R *stale = (R *)G.stale;
     const R invn3 = (R)(1.0 / (double)g.nreal);
-    switch (k) {
-      case 0:
-        colpass<0, false>(G, st, jobs_pass_a(s == 0 ? SLOT_SA : SLOT_SB));
-        break;
-      case 1:
-        colpass<1, false>(G, st, jobs_pass_b(s == 0));
-        break;
-      case 2:
-        if (s == 0)
-          zpass<0>(G, st, work, stale, invn3);
-        else if (s < 3)
-          zpass<1>(G, st, work, stale, invn3);
-        else
-          zpass<2>(G, st, work, stale, invn3);
-        break;
-      case 3:
-      case 4: {
-        // D: y forward, E1: x forward (in place on the three N slots); only
-        // the modes inside the 2/3 rule are computed and stored
-        const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
-        ColJobs j = jobs_map(io, io, 3);
-        j.masked = 1;
-        if (k == 3)
-          colpass<1, true>(G, st, j);
-        else
-          colpass<0, true>(G, st, j);
-        break;
-      }
-      default: {
-        StageArgs<R> sa;
-        sa.u0 = slot(G, SLOT_SA);
-        sa.us = slot(G, s == 0 ? SLOT_SA : SLOT_SB);
-        sa.acc = slot(G, SLOT_ACC);
-        sa.next = slot(G, SLOT_SB);
-        sa.ph = (s == 3 && (G.flags & DNS_FLAG_PRESSURE)) ? slot(G, SLOT_P) : nullptr;
-        sa.coef = G.coef;
-        sa.a = RK_A[s];
-        sa.b = s < 3 ? RK_B[s] : 0.0;
-        const long long npad = (long long)N * N * g.nfp;
-        const int per = UPD_THREADS * UpdVec<R>::VP;
-        dim3 grid((unsigned)((npad + per - 1) / per), G.nruns);
-        switch (s) {
-          case 0: k_update<R, N, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          case 1: k_update<R, N, 1><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          case 2: k_update<R, N, 2><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-          default: k_update<R, N, 3><<<grid, UPD_THREADS, 0, st>>>(work, g, sa); break;
-        }
+    const PPhase<R> P = describe(G, s, k);
+    const dim3 grid(P.gx, P.gy, P.gz);
+    if (P.kind == PK_COL) {
+      ColFn f = P.axis == 0 ? (P.fwd ? colkern<0, true>() : colkern<0, false>())
+                            : (P.fwd ? colkern<1, true>() : colkern<1, false>());
+      f<<<grid, P.tpi, P.smem, st>>>((C *)G.S, (C *)G.S, tw(G), g, P.jobs);
+    } else if (P.kind == PK_Z) {
+      if (P.sub == 0)
+        zpass<0>(G, st, work, stale, invn3);
+      else if (P.sub == 1)
+        zpass<1>(G, st, work, stale, invn3);
+      else
+        zpass<2>(G, st, work, stale, invn3);
+    } else {
+      switch (s) {
+        case 0: k_update<R, N, 0><<<grid, UPD_THREADS, 0, st>>>(work, g, P.sa); break;
+        case 1: k_update<R, N, 1><<<grid, UPD_THREADS, 0, st>>>(work, g, P.sa); break;
+        case 2: k_update<R, N, 2><<<grid, UPD_THREADS, 0, st>>>(work, g, P.sa); break;
+        default: k_update<R, N, 3><<<grid, UPD_THREADS, 0, st>>>(work, g, P.sa); break;
       }
     }
+  }
+
+  // this group's part of the persistent ensemble kernel's plan
+  static void plan_group(const Group &G, PGroup<R> &pg) {
+    pg.n = N;
+    pg.g = G.g;
+    pg.S = (C *)G.S;
+    pg.work = slot(G, SLOT_WORK);
+    pg.stale = (R *)G.stale;
+    pg.tw = tw(G);
+    pg.invn3 = (R)(1.0 / (double)G.g.nreal);
+    for (int s = 0; s < 4; s++)
+      for (int k = 0; k < KERNELS_PER_STAGE; k++) pg.ph[s * KERNELS_PER_STAGE + k] = describe(G, s, k);
   }
 
   static void step(const Group &G, cudaStream_t st) {
@@ -1198,10 +1260,159 @@ int dns_time_kernels(dns_ctx *c, double nu, double dt, long nsteps, double *ms) 
 /* ensemble                                                            */
 /* ------------------------------------------------------------------ */
 
+static int ens_build_graph(dns_ens *e);
+extern "C++" {
+// ---- the persistent schedule ----
+static bool ens_persistent_supported(const dns_ens *e) {
+  if (e->groups.size() > (size_t)PMAXG) return false;
+  for (const Group &G : e->groups)
+    if (!p_supported_n(G.n)) return false;
+  return true;
+}
+
+template <class R>
+static int ens_build_persistent_t(dns_ens *e) {
+  PPlan<R> plan{};
+  plan.ngroups = (int)e->groups.size();
+  size_t smem = 0;
+  for (size_t q = 0; q < e->groups.size(); q++) {
+    const Group &G = e->groups[q];
+    dispatch(G, [&](auto ops) {
+      using O = decltype(ops);
+      if constexpr (std::is_same<typename O::Real, R>::value) O::plan_group(G, plan.gr[q]);
+    });
+    for (const PPhase<R> &P : plan.gr[q].ph) smem = std::max(smem, (size_t)(PBS / P.tpi) * P.smem);
+  }
+  int dev = 0, sms = 0, per = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(p_prepare<R>(smem, &per));
+  if (per < 1) return fail(DNS_ERR_UNSUPPORTED, "persistent ensemble kernel does not fit", __FILE__, __LINE__);
+  e->pgrid = per * sms;
+  e->psmem = smem;
+  CK(cudaMalloc(&e->pplan, sizeof plan));
+  CK(cudaMalloc((void **)&e->psync, sizeof(PSync)));
+  CK(cudaMemcpyAsync(e->pplan, &plan, sizeof plan, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemsetAsync(e->psync, 0, sizeof(PSync), e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return DNS_OK;
+}
+
+// limit of the persistent kernel's grid-barrier waits (a phase lasts
+// microseconds to milliseconds)
+constexpr unsigned long long P_WAIT_NS = 2000000000ull;
+
+template <class R>
+static cudaError_t ens_launch_persistent_t(dns_ens *e, cudaStream_t st) {
+  return p_launch<R>(e->pgrid, e->psmem, st, (const PPlan<R> *)e->pplan, e->psync, P_WAIT_NS);
+}
+
+static cudaError_t ens_launch_persistent(dns_ens *e, cudaStream_t st) {
+  return e->groups[0].precision == DNS_PREC_FP64 ? ens_launch_persistent_t<double>(e, st)
+                                                 : ens_launch_persistent_t<float>(e, st);
+}
+
+static int ens_build_persistent(dns_ens *e) {
+  int st = e->groups[0].precision == DNS_PREC_FP64 ? ens_build_persistent_t<double>(e)
+                                                   : ens_build_persistent_t<float>(e);
+  if (st != DNS_OK) return st;
+  // one step = one graph of the single cooperative launch, where the
+  // runtime captures it; else the launch itself
+  cudaGraph_t gr = nullptr;
+  e->pgraph_ok = false;
+  if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    cudaError_t le = ens_launch_persistent(e, e->stream);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &gr);
+    if (le == cudaSuccess && ce == cudaSuccess && gr &&
+        cudaGraphInstantiate(&e->pgraph, gr, 0) == cudaSuccess)
+      e->pgraph_ok = true;
+    if (gr) cudaGraphDestroy(gr);
+  }
+  cudaGetLastError();  // a refused capture leaves no error behind
+  return DNS_OK;
+}
+
+static int ens_step_persistent(dns_ens *e, long nsteps) {
+  for (long s = 0; s < nsteps; s++) {
+    if (e->pgraph_ok)
+      CK(cudaGraphLaunch(e->pgraph, e->stream));
+    else
+      CK(ens_launch_persistent(e, e->stream));
+  }
+  return DNS_OK;
+}
+
+static int ens_check_persistent(dns_ens *e) {
+  if (!e->psync) return DNS_OK;
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&err, &e->psync->err, sizeof err, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (err & PERR_BARRIER_TIMEOUT)
+    return fail(DNS_ERR_CUDA, "a grid-barrier wait of the persistent ensemble kernel timed out",
+                __FILE__, __LINE__);
+  return DNS_OK;
+}
+
+// ms per step of the current schedule: one untimed step, then 3 timed
+static int ens_time_steps(dns_ens *e, float *ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  CK(cudaEventCreate(&a));
+  cudaError_t ce = cudaEventCreate(&b);
+  int st = ce == cudaSuccess ? DNS_OK : fail(DNS_ERR_CUDA, cudaGetErrorString(ce), __FILE__, __LINE__);
+  auto one = [&]() -> int {
+    if (e->mode == 1) return ens_step_persistent(e, 1);
+    CK(cudaGraphLaunch(e->graph, e->stream));
+    return DNS_OK;
+  };
+  if (st == DNS_OK) st = one();
+  if (st == DNS_OK && (ce = cudaEventRecord(a, e->stream)) != cudaSuccess)
+    st = fail(DNS_ERR_CUDA, cudaGetErrorString(ce), __FILE__, __LINE__);
+  for (int i = 0; i < 3 && st == DNS_OK; i++) st = one();
+  if (st == DNS_OK && (ce = cudaEventRecord(b, e->stream)) == cudaSuccess &&
+      (ce = cudaEventSynchronize(b)) == cudaSuccess)
+    ce = cudaEventElapsedTime(ms, a, b);
+  if (st == DNS_OK && ce != cudaSuccess) st = fail(DNS_ERR_CUDA, cudaGetErrorString(ce), __FILE__, __LINE__);
+  if (st == DNS_OK) st = ens_check_persistent(e);
+  *ms /= 3.f;
+  cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  return st;
+}
+
+// The ensemble autotuner: time both schedules on the fresh (all-zero) state,
+// which every step keeps at zero, and keep the faster; the flags can force
+// either.  A persistent schedule exists when every size group is one the
+// persistent kernel compiles (32, 64, 128) and there are at most PMAXG.
+static int ens_choose_schedule(dns_ens *e, unsigned flags) {
+  const bool can = ens_persistent_supported(e);
+  if ((flags & DNS_FLAG_ENS_PERSISTENT) && !can)
+    return fail(DNS_ERR_UNSUPPORTED, "no persistent schedule for these grid sizes", __FILE__, __LINE__);
+  int st = DNS_OK;
+  const bool want_b = !(flags & DNS_FLAG_ENS_PERSISTENT);
+  const bool want_p = can && !(flags & DNS_FLAG_ENS_BATCHED);
+  if (want_b) {
+    e->mode = 0;
+    st = ens_build_graph(e);
+    if (st == DNS_OK && want_p) st = ens_time_steps(e, &e->step_ms[0]);
+  }
+  if (st == DNS_OK && want_p) {
+    e->mode = 1;
+    st = ens_build_persistent(e);
+    if (st == DNS_OK && want_b) st = ens_time_steps(e, &e->step_ms[1]);
+  }
+  if (st == DNS_OK && want_b && want_p) e->mode = e->step_ms[1] < e->step_ms[0] ? 1 : 0;
+  return st;
+}
+
+}  // extern "C++"
+
 int dns_ens_destroy(dns_ens *e) {
   if (!e) return DNS_OK;
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->pgraph) cudaGraphExecDestroy(e->pgraph);
+  if (e->pplan) cudaFree(e->pplan);
+  if (e->psync) cudaFree(e->psync);
   for (auto &G : e->groups) group_free(G);
   for (auto s : e->gstreams) cudaStreamDestroy(s);
   for (auto v : e->gevents) cudaEventDestroy(v);
@@ -1251,6 +1462,7 @@ int dns_ens_create(int nruns, const long *n, int precision, unsigned flags, dns_
       if (ev) e->gevents.push_back(ev);
     }
   }
+  if (st == DNS_OK) st = ens_choose_schedule(e, flags);
   if (st != DNS_OK) {
     std::string keep = g_last_error;
     dns_ens_destroy(e);
@@ -1337,9 +1549,50 @@ int dns_ens_step(dns_ens *e, long nsteps) {
     if (!e->have_state[r]) return fail(DNS_ERR_STATE, "a run has no velocity", __FILE__, __LINE__);
   if (!e->params_set) return fail(DNS_ERR_STATE, "nu and dt not set", __FILE__, __LINE__);
   if (nsteps == 0) return DNS_OK;
+  if (e->mode == 1) return ens_step_persistent(e, nsteps);
   int st = ens_build_graph(e);
   if (st != DNS_OK) return st;
   for (long s = 0; s < nsteps; s++) CK(cudaGraphLaunch(e->graph, e->stream));
+  return DNS_OK;
+}
+
+int dns_ens_get_schedule(dns_ens *e, char *buf, long len) {
+  if (!e || !buf || len < 1) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  std::string s = e->mode == 1 ? "persistent" : "batched";
+  char tmp[256];
+  snprintf(tmp, sizeof tmp,
+           " (ms per step: batched %.4f, persistent %.4f, -1 = not timed; persistent grid %d "
+           "blocks of %d threads, %zu B shared, %s)",
+           (double)e->step_ms[0], (double)e->step_ms[1], e->pgrid, PBS, e->psmem,
+           e->pgraph_ok ? "graph-captured" : (e->pplan ? "direct launch" : "not built"));
+  s += tmp;
+  for (const Group &G : e->groups) {
+    std::string g;
+    dispatch(G, [&](auto ops) { g = decltype(ops)::schedule(); });
+    snprintf(tmp, sizeof tmp, "; n=%ld: ", G.n);
+    s += tmp + g;
+  }
+  snprintf(buf, (size_t)len, "%s", s.c_str());
+  return DNS_OK;
+}
+
+int dns_selftest_barrier_timeout(double limit_s, int *timed_out) {
+  if (!timed_out || !(limit_s > 0.0) || limit_s > 10.0)
+    return fail(DNS_ERR_ARG, "limit_s must be in (0, 10]", __FILE__, __LINE__);
+  *timed_out = 0;
+  cudaStream_t st = nullptr;
+  PSync *d = nullptr;
+  PSync h{};
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaError_t e = cudaMalloc((void **)&d, sizeof(PSync));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(PSync), st);
+  if (e == cudaSuccess) e = p_barrier_selftest(d, st, (unsigned long long)(limit_s * 1e9));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (d) cudaFree(d);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) return fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+  *timed_out = (h.err & PERR_BARRIER_TIMEOUT) ? 1 : 0;
   return DNS_OK;
 }
 
@@ -1357,6 +1610,8 @@ int dns_ens_diagnostics(dns_ens *e, double *out) {
     base += G.nruns;
   }
   CK(cudaStreamSynchronize(e->stream));
+  const int pst = ens_check_persistent(e);
+  if (pst != DNS_OK) return pst;
   bool finite = true;
   for (int r = 0; r < e->nruns; r++) {
     const double4 v = e->diag_host[gbase[e->run_group[r]] + e->run_index[r]];
@@ -1382,7 +1637,7 @@ void *dns_ens_get_stream(dns_ens *e) { return e ? (void *)e->stream : nullptr; }
 int dns_ens_synchronize(dns_ens *e) {
   if (!e) return fail(DNS_ERR_ARG, "NULL ensemble", __FILE__, __LINE__);
   CK(cudaStreamSynchronize(e->stream));
-  return DNS_OK;
+  return ens_check_persistent(e);
 }
 
 /* ------------------------------------------------------------------ */

@@ -50,11 +50,15 @@ enum {
  * Host-side arrays are float64 for both. */
 enum { DNS_PREC_FP64 = 0, DNS_PREC_MIXED = 1 };
 
-/* flags for dns_create */
+/* flags for dns_create (and dns_ens_create) */
 enum {
-  DNS_FLAG_PRESSURE = 1u /* keep the pressure P_hat of the last RK stage so
-                            that dns_get_fields can return P (needed by the
-                            -d dump, main.c:269-279) */
+  DNS_FLAG_PRESSURE = 1u, /* keep the pressure P_hat of the last RK stage so
+                             that dns_get_fields can return P (needed by the
+                             -d dump, main.c:269-279) */
+  /* dns_ens_create only: force the ensemble's schedule instead of letting
+   * its autotuner time both (see dns_ens_create) */
+  DNS_FLAG_ENS_BATCHED = 2u,
+  DNS_FLAG_ENS_PERSISTENT = 4u
 };
 
 typedef struct dns_ctx dns_ctx;
@@ -162,12 +166,32 @@ int dns_time_kernels(dns_ctx *ctx, double nu, double dt, long nsteps, double *ms
 /* ---- ensemble: many independent runs stepped together ----
  * No counterpart in the reference's main loop; it generalises its
  * process-level ensembles (run.sh / hal.sh run one dns per core).  Runs of
- * equal n share batched kernel launches; groups of different n run
- * concurrently; one CUDA graph launch advances every run by one RK4 step.
- * Each run follows main.c's step exactly (stale velocity included). */
+ * any grid sizes and viscosities advance together, each following main.c's
+ * step exactly (stale velocity included), under one of two schedules:
+ *   batched     runs of equal n share batched kernel launches (24 per step),
+ *               groups of different n run as concurrent branches of one
+ *               CUDA graph launch per step;
+ *   persistent  one cooperative kernel launch per step (captured in a CUDA
+ *               graph) walks the 24 passes of every run of every size, the
+ *               passes separated by grid-wide barriers (grid sizes 32, 64
+ *               and 128, at most four distinct sizes).
+ * Both give bit-identical states.  dns_ens_create times both on the fresh
+ * ensemble and keeps the faster (its autotuner) unless a flag forces one:
+ * DNS_FLAG_ENS_BATCHED or DNS_FLAG_ENS_PERSISTENT (DNS_ERR_UNSUPPORTED when
+ * the sizes have no persistent schedule).  A barrier wait of the persistent
+ * kernel that runs past its limit (2 s) makes the kernel end and the next
+ * dns_ens_synchronize / dns_ens_diagnostics return DNS_ERR_CUDA. */
 typedef struct dns_ens dns_ens;
 /* nruns runs, run r of grid size n[r] (same precision and flags for all) */
 int dns_ens_create(int nruns, const long *n, int precision, unsigned flags, dns_ens **out);
+/* the schedule the ensemble runs (and the timings that chose it), text of
+ * at most len bytes */
+int dns_ens_get_schedule(dns_ens *e, char *buf, long len);
+/* Self-test of the persistent kernel's bounded barrier wait (no counterpart
+ * in the reference): a grid barrier that one block never reaches must give
+ * up after limit_s seconds (0 < limit_s <= 10) and report it in the error
+ * word; *timed_out = 1 when it did. */
+int dns_selftest_barrier_timeout(double limit_s, int *timed_out);
 int dns_ens_destroy(dns_ens *e);
 /* initial velocity of one run (as dns_set_velocity) */
 int dns_ens_set_velocity(dns_ens *e, int run, const double *U, const double *V, const double *W);
