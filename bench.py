@@ -273,6 +273,28 @@ def ensemble_leg(steps: int, warmup: int):
         ms = e0.elapsed_time(e1)
         d = ens.diagnostics(allow_nonfinite=True)
         finite = all(np.isfinite(float(a)) and np.isfinite(float(b)) for a, b in d)
+        schedule = ens.schedule()
+    # the other schedule of the ensemble autotuner, timed the same way
+    other = {}
+    chosen = schedule.split(" ")[0]
+    flag = dns_b200.DNS_FLAG_ENS_PERSISTENT if chosen == "batched" else dns_b200.DNS_FLAG_ENS_BATCHED
+    with dns_b200.Ensemble(sizes, prec, flag) as eo:
+        so = torch.cuda.ExternalStream(eo.stream)
+        for r in range(len(sizes)):
+            eo.set_perturbed_tgv(r, seed=r, amplitude=1e-3)
+        eo.set_params(nus, dt)
+        eo.step(warmup)
+        eo.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(so)
+        eo.step(min(steps, 100))
+        b.record(so)
+        b.synchronize()
+        oms = a.elapsed_time(b) / min(steps, 100)
+        eo.synchronize()
+        other = {"schedule": "persistent" if chosen == "batched" else "batched",
+                 "ms_per_ensemble_step": oms, "value": len(sizes) / (oms / 1000.0)}
     seq_ms = {}
     for n in (64, 128):
         with dns_b200.Context(n, prec) as c:
@@ -303,7 +325,8 @@ def ensemble_leg(steps: int, warmup: int):
             "bytes_per_ensemble_step": ens_bytes,
             "roofline_frac": ens_bytes * ens_sps / (peak * 1e9),
             "frac_of_model_roofline": ens_model * ens_sps / (peak * 1e9),
-            "peak_source": peak_kind}
+            "peak_source": peak_kind, "schedule": schedule.split(" (")[0],
+            "autotuner": schedule.split("; n=")[0], "other_schedule": other}
 
 
 def n512_leg(steps: int, warmup: int):
@@ -614,6 +637,7 @@ def main() -> int:
             "adjoint": adj,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "schedule": ctx.schedule(),
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -281,8 +281,14 @@ struct Ops {
   // ---- autotuner of the column-pass register schedules ----
   template <int AXIS, bool FWD>
   static cudaError_t time_cands(const Group &G1, cudaStream_t st, const ColJobs &jobs,
-                                cudaEvent_t e0, cudaEvent_t e1, int force) {
+                                cudaEvent_t e0, cudaEvent_t e1, int force, int force_m) {
     constexpr int n = Cands<AXIS>::n;
+    if (force_m >= 0) {  // a given register schedule: its candidate, else the compiler's
+      col_pick[AXIS][FWD] = 0;
+      for (int i = 0; i < n; i++)
+        if (Cands<AXIS>::m[i] == force_m) col_pick[AXIS][FWD] = i;
+      return cudaSuccess;
+    }
     int best = 0;
     for (int i = 0; i < n; i++) {
       col_pick[AXIS][FWD] = i;
@@ -307,7 +313,11 @@ struct Ops {
   // (their real job tables, on the work slots of run 0, whose contents do
   // not matter to an FFT's timing) and keep the fastest of each; once per
   // process and size.  DNS_B200_TUNE=0 keeps the compiler's schedule,
-  // DNS_B200_TUNE=f<k> forces candidate k (the last where there are fewer).
+  // DNS_B200_TUNE=f<k> forces candidate k (the last where there are fewer),
+  // DNS_B200_TUNE=m<a>,<b>,<c>,<d> the schedules of min blocks/SM a, b, c, d
+  // for the x inverse, x forward, y inverse and y forward passes (as
+  // dns_get_schedule reports them; a value that is not a candidate means
+  // the compiler's).
   static cudaError_t tune(const Group &G, cudaStream_t st, bool *ran) {
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
@@ -319,6 +329,15 @@ struct Ops {
       return cudaSuccess;
     }
     const int force = (env && env[0] == 'f') ? atoi(env + 1) : -1;
+    int fm[4] = {-1, -1, -1, -1};  // x inverse, x forward, y inverse, y forward
+    if (env && env[0] == 'm') {
+      const char *c = env + 1;
+      for (int i = 0; i < 4 && *c; i++) {
+        fm[i] = atoi(c);
+        while (*c && *c != ',') c++;
+        if (*c == ',') c++;
+      }
+    }
     const Group G1 = G.one(0);
     const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
     ColJobs jm = jobs_map(io, io, 3);
@@ -326,10 +345,11 @@ struct Ops {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    if (e == cudaSuccess) e = time_cands<0, false>(G1, st, jobs_pass_a(SLOT_WORK), e0, e1, force);
-    if (e == cudaSuccess) e = time_cands<1, false>(G1, st, jobs_pass_b(false), e0, e1, force);
-    if (e == cudaSuccess) e = time_cands<1, true>(G1, st, jm, e0, e1, force);
-    if (e == cudaSuccess) e = time_cands<0, true>(G1, st, jm, e0, e1, force);
+    if (e == cudaSuccess)
+      e = time_cands<0, false>(G1, st, jobs_pass_a(SLOT_WORK), e0, e1, force, fm[0]);
+    if (e == cudaSuccess) e = time_cands<1, false>(G1, st, jobs_pass_b(false), e0, e1, force, fm[2]);
+    if (e == cudaSuccess) e = time_cands<1, true>(G1, st, jm, e0, e1, force, fm[3]);
+    if (e == cudaSuccess) e = time_cands<0, true>(G1, st, jm, e0, e1, force, fm[1]);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (e == cudaSuccess) tuned = true;

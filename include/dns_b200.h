@@ -42,11 +42,11 @@ enum {
 
 /* precision of a context:
  *   DNS_PREC_FP64   everything in float64 (the reference's arithmetic);
- *   DNS_PREC_MIXED  fields, FFTs and the nonlinear term in float32 (twiddles
- *                   generated in float64/long double and rounded once); the
- *                   energy/enstrophy reductions (double-double) and the
- *                   pointwise update with its viscous and time-step
- *                   coefficients computed in float64, stored in float32.
+ *   DNS_PREC_MIXED  fields, FFTs, the nonlinear term, the projection and the
+ *                   RK axpys in float32 (twiddles generated in long double
+ *                   and rounded once); the energy/enstrophy reductions
+ *                   (double-double) and the viscous coefficient nu dt |k|^2
+ *                   in float64, the latter rounded once per point.
  * Host-side arrays are float64 for both. */
 enum { DNS_PREC_FP64 = 0, DNS_PREC_MIXED = 1 };
 
@@ -146,7 +146,10 @@ int dns_get_info(dns_ctx *ctx, dns_info_t *info);
  * timing every compiled candidate once per process, with the measured
  * times.  All candidates compute bit-identical results.  The environment
  * variable DNS_B200_TUNE=0 keeps the compiler's schedule; DNS_B200_TUNE=f<k>
- * forces candidate k.  Writes a NUL-terminated text of at most len bytes. */
+ * forces candidate k; DNS_B200_TUNE=m<a>,<b>,<c>,<d> the schedules of a, b,
+ * c, d min blocks/SM for the x inverse, x forward, y inverse and y forward
+ * passes (to reproduce a reported choice, e.g. under a profiler).  Writes a
+ * NUL-terminated text of at most len bytes. */
 int dns_get_schedule(dns_ctx *ctx, char *buf, long len);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time work

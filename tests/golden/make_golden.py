@@ -24,6 +24,9 @@ Fixtures written:
   refrun_tgv128_re3000_dt0.0025_T2.5.txt
       the same at nu = 1/3000, T = 2.5 (1000 steps), for the GPU test of the
       128^3 path against main.c past t = 1.
+  refrun_tgv128_re1600_dt0.005_T10.txt
+      the 128^3 configuration of the mixed-precision comparison: nu = 1/1600,
+      dt = 0.005, T = 10 (2000 steps).
 """
 import argparse
 import hashlib
@@ -61,7 +64,8 @@ def main() -> int:
         runs = ((6, "0.01", "0.01", "1", "refrun_tgv64_nu0.01_dt0.01_T1.txt"),
                 (5, "0.01", "0.01", "0.2", "refrun_tgv32_nu0.01_dt0.01_T0.2.txt"),
                 (7, "%.16e" % (1 / 100), "0.0025", "5", "refrun_tgv128_re0100_dt0.0025_T5.txt"),
-                (7, "%.16e" % (1 / 3000), "0.0025", "2.5", "refrun_tgv128_re3000_dt0.0025_T2.5.txt"))
+                (7, "%.16e" % (1 / 3000), "0.0025", "2.5", "refrun_tgv128_re3000_dt0.0025_T2.5.txt"),
+                (7, "%.16e" % (1 / 1600), "0.005", "10", "refrun_tgv128_re1600_dt0.005_T10.txt"))
         for level, nu, dt, T, name in runs:
             raw = os.path.join(tmp, f"tgv{level}.raw")
             if not os.path.exists(raw):

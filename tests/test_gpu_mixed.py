@@ -1,14 +1,18 @@
 """GPU tests of the mixed-precision path (DNS_PREC_MIXED): float32 fields,
-FFTs and nonlinear term; float64 reductions and update coefficients.
+FFTs, nonlinear term and RK axpys; float64 reductions and viscous /
+time-step coefficients.
 
 Tolerances are float32 ones: transforms and single steps 1e-5 relative;
-the energy history of the 128^3 Taylor-Green run over t in [0, 10]
-(nu = 1/1600, dt = 0.005, 2000 steps) within 1e-5 relative of the FP64 path.
+the energy and enstrophy histories of the 128^3 Taylor-Green run over
+t in [0, 10] (nu = 1/1600, dt = 0.005) within 1e-5 relative of the FP64
+path and of main.c's own run, the final fields within 1e-4 relative L2.
 """
+import os
+
 import numpy as np
 import pytest
 
-from conftest import random_field
+from conftest import GOLDEN, read_history, random_field
 
 pytestmark = pytest.mark.gpu
 
@@ -58,30 +62,52 @@ def test_mixed_steps_match_oracle(dns, oracle_lib, n, steps):
     assert abs(E - Eo) <= F32_TOL * Eo and abs(Om - Oo) <= F32_TOL * Oo
 
 
-def history(dns, n, prec, nu, dt, nsteps):
+def run_config(dns, n, prec, nu, dt, T):
+    """main.c's loop for (T, dt): the printed (E, Omega) history and the
+    final spectral velocity and real fields."""
+    sched, total = dns.step_schedule(T, dt)
     U, V, W, _ = dns.tgv_fields(n)
     E, Om = [], []
     with dns.Context(n, prec) as ctx:
         ctx.set_velocity(U, V, W)
-        for q in range(nsteps // 10 + 1):
-            if q:
-                ctx.step(nu, dt, 10)
+        done = 0
+        for tstep, _ in sched:
+            ctx.step(nu, dt, tstep - done)
+            done = tstep
             e, w = ctx.diagnostics()
-            E.append(float(e))
-            Om.append(float(w))
-    return np.array(E), np.array(Om)
+            E.append(e)
+            Om.append(w)
+        ctx.step(nu, dt, total - done)
+        uh, fields = ctx.get_spectral(), np.stack(ctx.get_fields())
+    return (np.array(E, dtype=np.longdouble), np.array(Om, dtype=np.longdouble), uh, fields,
+            [s for s, _ in sched])
 
 
-def test_mixed_tgv128_energy_error_over_t10(dns):
+def test_mixed_tgv128_config_against_fp64_and_main_c(dns):
     """Config: 128^3 Taylor-Green, nu = 1/1600, dt = 0.005, t in [0, 10]
-    (2000 steps).  Energy of the mixed path within 1e-5 of the FP64 path at
-    every printed step; the enstrophy error is reported."""
-    n, nu, dt = 128, 1.0 / 1600, 0.005
-    E64, O64 = history(dns, n, dns.DNS_PREC_FP64, nu, dt, 2000)
-    E32, O32 = history(dns, n, dns.DNS_PREC_MIXED, nu, dt, 2000)
-    de = np.abs(E32 - E64) / E64
-    do = np.abs(O32 - O64) / O64
-    print(f"\nmixed vs fp64, 128^3 Re=1600 dt=0.005 t<=10: max rel err E {de.max():.3e}, "
-          f"Omega {do.max():.3e}")
-    assert de.max() <= 1e-5, de.max()
-    assert do.max() <= 1e-3, do.max()
+    (2000 steps).  Per diagnostic: the FP64 path follows
+    main.c itself (oracle/_ref, the reference source compiled unchanged; its
+    stdout is the fixture) to 1e-12 on every printed line, and the mixed path
+    stays within 1e-5 relative of both in energy and enstrophy.  Per field:
+    the mixed path's final velocity (spectral and real) against the FP64
+    path's, relative L2, within 1e-4 (measured 4.5e-5: at t = 10 the flow
+    has become sensitive enough to amplify FP32 rounding; the diagnostics
+    stay at 3e-6)."""
+    n, nu, dt, T = 128, float("%.16e" % (1.0 / 1600)), 0.005, 10.0
+    steps, _, Eg, Og = read_history(os.path.join(GOLDEN, "refrun_tgv128_re1600_dt0.005_T10.txt"))
+    E64, O64, uh64, f64, s64 = run_config(dns, n, dns.DNS_PREC_FP64, nu, dt, T)
+    E32, O32, uh32, f32, _ = run_config(dns, n, dns.DNS_PREC_MIXED, nu, dt, T)
+    assert list(steps) == s64
+    rel = lambda a, b: np.abs(a - b) / np.abs(b)
+    e64, o64 = rel(E64, Eg).max(), rel(O64, Og).max()
+    e32, o32 = rel(E32, E64).max(), rel(O32, O64).max()
+    e32g, o32g = rel(E32, Eg).max(), rel(O32, Og).max()
+    fu = float(np.linalg.norm(uh32 - uh64) / np.linalg.norm(uh64))
+    fr = [float(np.linalg.norm(f32[c] - f64[c]) / np.linalg.norm(f64[c])) for c in range(2)]
+    print(f"\n128^3 Re=1600 dt=0.005 t<=10: fp64 vs main.c E {float(e64):.2e} Om {float(o64):.2e}; "
+          f"mixed vs fp64 E {float(e32):.2e} Om {float(o32):.2e}; mixed vs main.c E {float(e32g):.2e} "
+          f"Om {float(o32g):.2e}; final fields mixed vs fp64: spectral {fu:.2e}, U {fr[0]:.2e}, V {fr[1]:.2e}")
+    assert e64 <= 1e-12 and o64 <= 1e-12, (float(e64), float(o64))
+    assert e32 <= 1e-5 and o32 <= 1e-5, (float(e32), float(o32))
+    assert e32g <= 1e-5 and o32g <= 1e-5, (float(e32g), float(o32g))
+    assert fu <= 1e-4 and max(fr) <= 1e-4, (fu, fr)
