@@ -606,6 +606,15 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
     return ld(pOMZ, s);
   };
   auto f_zero = [&](int) -> C { return czero<C>(); };
+  // L2 prefetch of a row of `bytes` starting on a 128-byte line: the next
+  // pair's inputs are on their way from DRAM while this pair's FFT runs
+  // (the waits on those loads were the pass's largest stall)
+  auto pf = [&](const void *row, int bytes) {
+    if (!ok) return;
+    for (int l = t; l * 128 < bytes; l += T)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"((const char *)row + l * 128));
+  };
+  constexpr int ROWB = (N / 2 + 1) * (int)sizeof(C), REALB = N * (int)sizeof(R);
   const LineSync<(T > 32), BSync> sync{bsync};
   const PadShift<Z::PADSH> idx{};
   const long long roff = line * N;
@@ -616,6 +625,10 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
     // stale real velocity read where it is needed (L1/L2 hits the second time)
     auto sv = [&](int f, int e) -> R { return ok ? stale[f * g.nreal + roff + t + T * e] : R(0); };
     ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
+    pf(pOMZ, ROWB);
+    pf(stale + roff, REALB);
+    pf(stale + g.nreal + roff, REALB);
+    pf(stale + 2 * g.nreal + roff, REALB);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -667,6 +680,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       a = uu;
       b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
     });
+    pf(pW, ROWB);
+    pf(pOMZ, ROWB);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -680,6 +695,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       a = ld(pW, s);
       b = ld(pOMZ, s);
     });
+    pf(pV, ROWB);
+    pf(pDWDY, ROWB);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -728,6 +745,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       a = uu;
       b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
     });
+    pf(pW, ROWB);
+    pf(pOMZ, ROWB);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -740,6 +759,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       a = ld(pW, s);
       b = ld(pOMZ, s);
     });
+    pf(pV, ROWB);
+    pf(pDWDY, ROWB);
     line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
     R w[E], oz[E];
 #pragma unroll
