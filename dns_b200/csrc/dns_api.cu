@@ -339,7 +339,7 @@ struct Ops {
       }
     }
     const Group G1 = G.one(0);
-    const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+    const int io[3] = {SLOT_WORK + SNX, SLOT_WORK + SNY, SLOT_WORK + SNZ};
     ColJobs jm = jobs_map(io, io, 3);
     jm.masked = 1;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -428,7 +428,7 @@ struct Ops {
       } else {
         // D: y forward, E1: x forward (in place on the three N slots); only
         // the modes inside the 2/3 rule are computed and stored
-        const int io[3] = {SLOT_WORK + SU, SLOT_WORK + SV, SLOT_WORK + SW};
+        const int io[3] = {SLOT_WORK + SNX, SLOT_WORK + SNY, SLOT_WORK + SNZ};
         P.jobs = jobs_map(io, io, 3);
         P.jobs.masked = 1;
       }

@@ -38,8 +38,11 @@
 namespace dnsb {
 
 // work slots of the stage (after pass B, SOMZ holds omega_z = dv/dx - du/dy;
-// after pass A it holds dv/dx)
-enum { SU = 0, SV = 1, SW = 2, SOMZ = 3, SDWDX = 4, SDWDY = 5, NWORK = 6 };
+// after pass A it holds dv/dx).  The z pass writes N = u x omega over the
+// slots SNX, SNY, SNZ (those of u, v and dw/dy), each once the line's input
+// in it has been read, and D, E1 and E2 take N from there.
+enum { SU = 0, SV = 1, SDWDY = 2, SOMZ = 3, SDWDX = 4, SW = 5, NWORK = 6 };
+enum { SNX = 0, SNY = 1, SNZ = 2 };
 
 struct Geo {
   int n, nf, nfp;
@@ -439,28 +442,33 @@ struct ZC {
   static constexpr int E = P::E;
   static constexpr int T = N / E;                 // threads per line
   static constexpr int M = N / 2;
-  // FP64 with 16 values per thread: N_x, N_y, N_z stay in registers (up to
-  // 255 of them, 64-thread blocks); in the middle and last stages (u,
-  // omega_y), then (w, omega_z), wait in shared memory for the next pair's
-  // FFT, and the first stage reads the stale velocity where it needs it
+  // FP64 with 16 values per thread (S2) and FP32: the pairs run in the
+  // order (u, omega_y), (v, omega_x), (w, omega_z), so that N_z is complete
+  // after the second and goes through its forward FFT and out before the
+  // third; N_x and N_y are then formed in place in the FFT registers.  At
+  // most two fields beyond the FFT's own values are live: FP64 keeps (u,
+  // omega_y) in shared memory and (v, omega_x) in registers (64-thread
+  // blocks, 4 per SM: capping the registers for 5 or 6 blocks measured
+  // slower); FP32 keeps both pairs in registers (128 of them).  The first
+  // stage reads the stale velocity where it needs it.
   static constexpr bool S2 = sizeof(R) == 8 && E >= 16;
-  // FP32: N in registers in every stage (half the registers of FP64)
   static constexpr bool F32 = sizeof(R) == 4;
   static constexpr int WANT = S2 ? 64 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
-  // blocks per SM: register cap 255 (FP64), 128 (FP32 first stage, which
-  // keeps no velocity in registers), 170 (other FP32 stages)
-  static constexpr int MINB = S2 ? 4 : (F32 && KIND == 0) ? 4 : 3;
+  static constexpr int MINB = S2 ? 4 : F32 ? 4 : 3;  // blocks per SM
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
-  // staged scalars per line: S2 none (first stage), two (middle stage) or
-  // three (last stage, u kept for the stale store); FP32 none; FP64 with 8
-  // values per thread none (middle stage) or u, v, w, N_y, N_z
+  // stage twiddle entries held (even, so the exchange buffers stay 16-byte
+  // aligned)
+  static constexpr int TWN = (StageTw<P>::SIZE + 1) / 2 * 2 > 2 ? (StageTw<P>::SIZE + 1) / 2 * 2 : 2;
+  // staged scalars per line: S2 none (first stage) or (u, omega_y); FP32
+  // none; FP64 with 8 values per thread none (middle stage) or u, v, w,
+  // N_y, N_z
   static constexpr int STASH =
-      S2 ? (KIND == 0 ? 0 : (KIND + 1) * N) : ((KIND == 1 || F32) ? 0 : 5 * N);
+      S2 ? (KIND == 0 ? 0 : 2 * N) : ((KIND == 1 || F32) ? 0 : 5 * N);
   static constexpr size_t SMEM =
-      (size_t)(N + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
+      (size_t)(TWN + LINES * XB) * sizeof(cx<R>) + (size_t)LINES * STASH * sizeof(R);
 };
 
 // Hermitian-extended pair  Y[k] = A_ext[k] + i B_ext[k]  at k = t + T*e.
@@ -520,27 +528,24 @@ __device__ __forceinline__ void ext_gen(C (&y)[ZC<R, N, KIND>::E], int t, FAB fa
   }
 }
 
-// The forward half of the z pass for one line: (N_x, N_y) as one complex
-// FFT, then N_z (main.c:378-380); only kz <= kcut is stored (N enters the
-// update through the 2/3 rule only).  `row` = the line's row of work slot 0.
+// The forward transforms of the z pass for one line (main.c:378-380); only
+// kz <= kcut is stored (N enters the update through the 2/3 rule only).
+// `row` = the line's row of work slot 0.
+// (N_x, N_y) held in y as one complex line: FFT, unpack, store into SNX,
+// SNY (ends with a barrier: the exchange buffer is free again)
 template <class R, int N, int KIND, class Idx, class Sync>
-__device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
-                                               const R (&nx)[ZC<R, N, KIND>::E],
-                                               const R (&ny)[ZC<R, N, KIND>::E],
-                                               const R (&nz)[ZC<R, N, KIND>::E], int t,
-                                               const cx<R> *tw, cx<R> *xb, Idx idx, Sync sync,
-                                               cx<R> *row, const Geo &g, bool ok) {
+__device__ __forceinline__ void zfwd_xy(cx<R> (&y)[ZC<R, N, KIND>::E], int t, const cx<R> *tw,
+                                        cx<R> *xb, Idx idx, Sync sync, cx<R> *row, const Geo &g,
+                                        bool ok) {
   using C = cx<R>;
   using Z = ZC<R, N, KIND>;
   constexpr int E = Z::E, T = Z::T, M = Z::M;
   const int KZ = g.kcut < M ? g.kcut : M;
-#pragma unroll
-  for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
   line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
 #pragma unroll
   for (int e = 0; e < E; e++) xb[idx(t + T * e)] = y[e];
   sync();
-  C *oU = row + SU * g.slot, *oV = row + SV * g.slot;
+  C *oU = row + SNX * g.slot, *oV = row + SNY * g.slot;
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
@@ -555,15 +560,40 @@ __device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
     }
   }
   sync();
-#pragma unroll
-  for (int e = 0; e < E; e++) y[e] = cmk<C>(nz[e], R(0));
+}
+// N_z held in y as (N_z, 0): FFT, store into SNZ
+template <class R, int N, int KIND, class Idx, class Sync>
+__device__ __forceinline__ void zfwd_z(cx<R> (&y)[ZC<R, N, KIND>::E], int t, const cx<R> *tw,
+                                       cx<R> *xb, Idx idx, Sync sync, cx<R> *row, const Geo &g,
+                                       bool ok) {
+  using C = cx<R>;
+  using Z = ZC<R, N, KIND>;
+  constexpr int E = Z::E, T = Z::T, M = Z::M;
+  const int KZ = g.kcut < M ? g.kcut : M;
   line_fft<N, typename Z::P, true>(y, t, tw, xb, idx, sync);
-  C *oW = row + SW * g.slot;
+  C *oW = row + SNZ * g.slot;
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
     const int k = t + T * e;
     if (k <= KZ && ok) oW[k] = y[e];
   }
+}
+// both, from N held in registers (the stages that complete N at the end)
+template <class R, int N, int KIND, class Idx, class Sync>
+__device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
+                                               const R (&nx)[ZC<R, N, KIND>::E],
+                                               const R (&ny)[ZC<R, N, KIND>::E],
+                                               const R (&nz)[ZC<R, N, KIND>::E], int t,
+                                               const cx<R> *tw, cx<R> *xb, Idx idx, Sync sync,
+                                               cx<R> *row, const Geo &g, bool ok) {
+  using C = cx<R>;
+  constexpr int E = ZC<R, N, KIND>::E;
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nx[e], ny[e]);
+  zfwd_xy<R, N, KIND>(y, t, tw, xb, idx, sync, row, g, ok);
+#pragma unroll
+  for (int e = 0; e < E; e++) y[e] = cmk<C>(nz[e], R(0));
+  zfwd_z<R, N, KIND>(y, t, tw, xb, idx, sync, row, g, ok);
 }
 
 // One block of the z pass: Z::LINES lines starting at line b.x * LINES of
@@ -576,12 +606,12 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
   using C = cx<R>;
   using Z = ZC<R, N, KIND>;
   constexpr int E = Z::E, T = Z::T;
-  C *tw = (C *)smem;  // stage twiddles of the z plan (<= N entries)
+  C *tw = (C *)smem;  // stage twiddles of the z plan (Z::TWN entries)
   build_stage_tw<N, typename Z::P>(tw, twg, N, b.tid, b.nt);
   bsync();
   const int lid = b.tid / T, t = b.tid % T;
-  C *xb = tw + N + lid * Z::XB;
-  R *st = (R *)(tw + N + Z::LINES * Z::XB) + lid * Z::STASH;
+  C *xb = tw + Z::TWN + lid * Z::XB;
+  R *st = (R *)(tw + Z::TWN + Z::LINES * Z::XB) + lid * Z::STASH;
   // own points of staged field f: st[(f * E + e) * T + t]
   auto SU_ = [&](int f, int e) -> R & { return st[(f * E + e) * T + t]; };
   const long long line = (long long)b.x * Z::LINES + lid;
@@ -620,33 +650,102 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
   const long long roff = line * N;
 
   C y[E];
-  R nx[E], ny[E], nz[E];
-  if (KIND == 0 && (Z::S2 || Z::F32)) {
-    // stale real velocity read where it is needed (L1/L2 hits the second time)
-    auto sv = [&](int f, int e) -> R { return ok ? stale[f * g.nreal + roff + t + T * e] : R(0); };
-    ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
-    pf(pOMZ, ROWB);
-    pf(stale + roff, REALB);
-    pf(stale + g.nreal + roff, REALB);
-    pf(stale + 2 * g.nreal + roff, REALB);
-    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+  if constexpr (Z::S2 || Z::F32) {
+    if constexpr (KIND == 0) {
+      // first stage: (omega_x, omega_y) with the stale real velocity read
+      // where it is needed (L1/L2 hits the second time); N_z is complete
+      // after this pair and leaves before (omega_z, 0)
+      auto sv = [&](int f, int e) -> R { return ok ? stale[f * g.nreal + roff + t + T * e] : R(0); };
+      R nx[E], ny[E];
+      ext_pair<R, N, KIND>(y, t, f_ox, f_oy);
+      pf(pOMZ, ROWB);
+      pf(stale + roff, REALB);
+      pf(stale + g.nreal + roff, REALB);
+      pf(stale + 2 * g.nreal + roff, REALB);
+      line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R ox = y[e].x * invn3, oy = y[e].y * invn3;
-      const R u = sv(0, e), v = sv(1, e), w = sv(2, e);
-      nx[e] = -w * oy;
-      ny[e] = w * ox;
-      nz[e] = u * oy - v * ox;
-    }
-    ext_pair<R, N, KIND>(y, t, f_oz, f_zero);
-    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+      for (int e = 0; e < E; e++) {
+        const R ox = y[e].x * invn3, oy = y[e].y * invn3;
+        const R u = sv(0, e), v = sv(1, e), w = sv(2, e);
+        nx[e] = -w * oy;
+        ny[e] = w * ox;
+        y[e] = cmk<C>(u * oy - v * ox, R(0));  // N_z
+      }
+      zfwd_z<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
+      ext_pair<R, N, KIND>(y, t, f_oz, f_zero);
+      line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R oz = y[e].x * invn3;
-      nx[e] += sv(1, e) * oz;
-      ny[e] -= sv(0, e) * oz;
+      for (int e = 0; e < E; e++) {
+        const R oz = y[e].x * invn3;
+        y[e] = cmk<C>(nx[e] + sv(1, e) * oz, ny[e] - sv(0, e) * oz);  // (N_x, N_y)
+      }
+      zfwd_xy<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
+    } else {
+      // middle and last stages: (u, omega_y), (v, omega_x): N_z = u oy - v ox
+      // leaves; (w, omega_z): N_x = v oz - w oy, N_y = w ox - u oz formed in
+      // place and leave.  The last stage stores the velocity as the next
+      // stale one as it comes.
+      R su[Z::S2 ? 1 : E], soy[Z::S2 ? 1 : E];  // FP32: (u, omega_y) in registers
+      auto U_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(0, e); else return su[e]; };
+      auto OY_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(1, e); else return soy[e]; };
+      ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+        const C uu = ld(pU, s), d = ld(pDWDX, s);
+        a = uu;
+        b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
+      });
+      pf(pV, ROWB);
+      pf(pDWDY, ROWB);
+      line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const R u = y[e].x * invn3, oy = y[e].y * invn3;
+        if constexpr (Z::S2) {
+          SU_(0, e) = u;
+          SU_(1, e) = oy;
+        } else {
+          su[e] = u;
+          soy[e] = oy;
+        }
+        if (KIND == 2 && ok) stale[roff + t + T * e] = u;
+      }
+      ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+        const C vv = ld(pV, s), d = ld(pDWDY, s);
+        a = vv;
+        b = cmk<C>(d.x + (R)s * vv.y, d.y - (R)s * vv.x);  // dw/dy - i kz v
+      });
+      pf(pW, ROWB);
+      pf(pOMZ, ROWB);
+      line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+      R sv_[E], sox[E];
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const R v = y[e].x * invn3, ox = y[e].y * invn3;
+        sv_[e] = v;
+        sox[e] = ox;
+        const R nz = U_(e) * OY_(e);
+        y[e] = cmk<C>(nz - v * ox, R(0));  // N_z
+        if (KIND == 2 && ok) stale[g.nreal + roff + t + T * e] = v;
+      }
+      zfwd_z<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
+      ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
+        a = ld(pW, s);
+        b = ld(pOMZ, s);
+      });
+      line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const R w = y[e].x * invn3, oz = y[e].y * invn3;
+        const R nx = -w * OY_(e), ny = -U_(e) * oz;
+        y[e] = cmk<C>(nx + sv_[e] * oz, ny + w * sox[e]);  // (N_x, N_y)
+        if (KIND == 2 && ok) stale[2 * g.nreal + roff + t + T * e] = w;
+      }
+      zfwd_xy<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
     }
-  } else if (KIND == 0) {
+  } else {
+    // FP64 with 8 values per thread (n <= 64): N in registers, forward
+    // transforms at the end
+    R nx[E], ny[E], nz[E];
+    if (KIND == 0) {
     // stale real velocity, own points m = t + T e
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -672,67 +771,7 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       nx[e] += SU_(1, e) * oz;
       ny[e] -= SU_(0, e) * oz;
     }
-  } else if (Z::S2) {
-    // the middle stage's pairs; u, omega_y and then w, omega_z are staged;
-    // the last stage also stores the velocity as the next stale one
-    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
-      const C uu = ld(pU, s), d = ld(pDWDX, s);
-      a = uu;
-      b = cmk<C>(-(R)s * uu.y - d.x, (R)s * uu.x - d.y);  // i kz u - dw/dx
-    });
-    pf(pW, ROWB);
-    pf(pOMZ, ROWB);
-    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R u = y[e].x * invn3, oy = y[e].y * invn3;
-      nz[e] = u * oy;
-      SU_(0, e) = u;
-      SU_(1, e) = oy;
-      if (KIND == 2) SU_(2, e) = u;
-    }
-    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
-      a = ld(pW, s);
-      b = ld(pOMZ, s);
-    });
-    pf(pV, ROWB);
-    pf(pDWDY, ROWB);
-    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R w = y[e].x * invn3, oz = y[e].y * invn3;
-      const R u = SU_(0, e), oy = SU_(1, e);
-      nx[e] = -w * oy;
-      ny[e] = -u * oz;
-      SU_(0, e) = w;
-      SU_(1, e) = oz;
-    }
-    ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
-      const C vv = ld(pV, s), d = ld(pDWDY, s);
-      a = vv;
-      b = cmk<C>(d.x + (R)s * vv.y, d.y - (R)s * vv.x);  // dw/dy - i kz v
-    });
-    line_fft<N, typename Z::P, false>(y, t, tw, xb, idx, sync);
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const R v = y[e].x * invn3, ox = y[e].y * invn3;
-      const R w = SU_(0, e), oz = SU_(1, e);
-      nx[e] += v * oz;
-      ny[e] += w * ox;
-      nz[e] -= v * ox;
-      if (KIND == 2) SU_(1, e) = v;
-    }
-    if (KIND == 2 && ok) {
-      // the velocity becomes the next step's stale one (u, v, w staged)
-#pragma unroll
-      for (int e = 0; e < E; e++) {
-        const long long m = roff + t + T * e;
-        stale[m] = SU_(2, e);
-        stale[g.nreal + m] = SU_(1, e);
-        stale[2 * g.nreal + m] = SU_(0, e);
-      }
-    }
-  } else if (KIND == 1 || Z::F32) {
+    } else if (KIND == 1) {
     // Pairs ordered so that every input slot is read once and the cross
     // product accumulates in registers (FP32 last stage: the velocity is
     // stored as the next stale one as it comes):
@@ -785,7 +824,7 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       nz[e] -= v * ox;
       if (KIND == 2 && ok) stale[g.nreal + roff + t + T * e] = v;
     }
-  } else {
+    } else {
     // FP64 last stage at 8 values per thread: the velocity is also stored as
     // the next stale one, so it is staged in shared memory (the register-only
     // order above spills here)
@@ -827,7 +866,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       }
     }
   }
-  zstage_forward<R, N, KIND>(y, nx, ny, nz, t, tw, xb, idx, sync, work + off, g, ok);
+    zstage_forward<R, N, KIND>(y, nx, ny, nz, t, tw, xb, idx, sync, work + off, g, ok);
+  }
 }
 
 template <class R, int N, int KIND>
