@@ -363,11 +363,12 @@ def n512_leg(steps: int, warmup: int):
 
 
 def adjoint_leg(n: int = 128, snapshots: int = 20):
-    """Discrete adjoint of the final energy (dns_adjoint_energy): 128^3
+    """Discrete adjoint of the final energy (dns_adjoint_energy_prec): 128^3
     unit-energy random isotropic field, nu = 0.005, dt = 0.005, T = 2
-    (401 steps), 20 snapshots.  Wall time of the whole call (forward sweep
-    with checkpoints, reverse sweep with recomputation, host copies of the
-    field and the gradient) per step, against the plain forward step."""
+    (401 steps), 20 snapshots, FP64 and mixed.  Wall time of the whole call
+    (forward sweep with checkpoints, reverse sweep with recomputation, host
+    copies of the field and the gradient) per step, against the plain
+    forward step of the same precision."""
     import numpy as np
 
     import dns_b200
@@ -378,22 +379,30 @@ def adjoint_leg(n: int = 128, snapshots: int = 20):
     with dns_b200.Context(n) as c:
         c.set_velocity(*u0)
         E0, _ = c.diagnostics()
-        s = float(1.0 / np.sqrt(E0))
-        u0 = [a * s for a in u0]
-        c.set_velocity(*u0)
-        c.step(nu, dt, 5)
-        c.synchronize()
+    s = float(1.0 / np.sqrt(E0))
+    u0 = [a * s for a in u0]
+    out = {"n": n, "steps": nsteps, "snapshots": snapshots}
+    for name, prec in (("fp64", dns_b200.DNS_PREC_FP64), ("mixed", dns_b200.DNS_PREC_MIXED)):
+        with dns_b200.Context(n, prec) as c:
+            c.set_velocity(*u0)
+            c.step(nu, dt, 5)
+            c.synchronize()
+            t0 = time.perf_counter()
+            c.step(nu, dt, nsteps)
+            c.synchronize()
+            fwd_ms = (time.perf_counter() - t0) * 1000.0 / nsteps
+        # warm-up (module load, plans)
+        dns_b200.adjoint_energy(*u0, nu, dt, 8, snapshots=4, precision=prec)
         t0 = time.perf_counter()
-        c.step(nu, dt, nsteps)
-        c.synchronize()
-        fwd_ms = (time.perf_counter() - t0) * 1000.0 / nsteps
-    dns_b200.adjoint_energy(*u0, nu, dt, 8, snapshots=4)  # warm-up (module load, plans)
-    t0 = time.perf_counter()
-    dns_b200.adjoint_energy(*u0, nu, dt, nsteps, snapshots=snapshots)
-    wall = time.perf_counter() - t0
-    return {"n": n, "steps": nsteps, "snapshots": snapshots, "wall_s": wall,
-            "ms_per_step": wall * 1000.0 / nsteps, "forward_ms_per_step": fwd_ms,
-            "vs_forward_step": wall * 1000.0 / nsteps / fwd_ms}
+        dns_b200.adjoint_energy(*u0, nu, dt, nsteps, snapshots=snapshots, precision=prec)
+        wall = time.perf_counter() - t0
+        leg = {"wall_s": wall, "ms_per_step": wall * 1000.0 / nsteps,
+               "forward_ms_per_step": fwd_ms, "vs_forward_step": wall * 1000.0 / nsteps / fwd_ms}
+        if name == "fp64":
+            out.update(leg)
+        else:
+            out["mixed"] = leg
+    return out
 
 
 def run_reference_arm(args, world, rank):

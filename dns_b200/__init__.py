@@ -95,6 +95,8 @@ _SIGS = {
     "dns_selftest_barrier_timeout": (ctypes.c_int, [_D, ctypes.POINTER(ctypes.c_int)]),
     "dns_adjoint_energy": (ctypes.c_int, [ctypes.c_long, _P, _P, _P, _D, _D, ctypes.c_long,
                                           ctypes.c_int, _P, _P, _P, _P, _P]),
+    "dns_adjoint_energy_prec": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, _P, _P, _P, _D, _D,
+                                               ctypes.c_long, ctypes.c_int, _P, _P, _P, _P, _P]),
 }
 
 
@@ -397,31 +399,34 @@ def perturbed_tgv(n: int, seed: int, amplitude: float = 1e-3, rng: str = "pcg64"
     return U + s * d[0], V + s * d[1], W + s * d[2]
 
 
-def adjoint_energy(U, V, W, nu: float, dt: float, nsteps: int, snapshots: int = 20):
-    """Final energy J = E(T) (main.c's definition) after `nsteps` FP64 RK4
-    steps from (U, V, W), and its gradient: (J, (dJ/dU, dJ/dV, dJ/dW), dJ/dnu).
-    The adjoint runs on the GPU (dns_adjoint_energy)."""
+def adjoint_energy(U, V, W, nu: float, dt: float, nsteps: int, snapshots: int = 20,
+                   precision: int = DNS_PREC_FP64):
+    """Final energy J = E(T) (main.c's definition) after `nsteps` RK4 steps
+    from (U, V, W), and its gradient: (J, (dJ/dU, dJ/dV, dJ/dW), dJ/dnu).
+    The adjoint runs on the GPU (dns_adjoint_energy_prec) in the given
+    precision (DNS_PREC_FP64 or DNS_PREC_MIXED)."""
     lib = load_library()
     U, V, W = _f64(U), _f64(V), _f64(W)
     n = round(U.size ** (1.0 / 3))
     g = [np.empty_like(U), np.empty_like(V), np.empty_like(W)]
     J, gnu = ctypes.c_double(), ctypes.c_double()
-    _check(lib.dns_adjoint_energy(n, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, snapshots,
-                                  ctypes.byref(J), _ptr(g[0]), _ptr(g[1]), _ptr(g[2]),
-                                  ctypes.byref(gnu)))
+    _check(lib.dns_adjoint_energy_prec(n, precision, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps,
+                                       snapshots, ctypes.byref(J), _ptr(g[0]), _ptr(g[1]),
+                                       _ptr(g[2]), ctypes.byref(gnu)))
     return J.value, tuple(a.reshape(U.shape) for a in g), gnu.value
 
 
-def final_energy(U, V, W, nu: float, dt: float, nsteps: int) -> float:
+def final_energy(U, V, W, nu: float, dt: float, nsteps: int,
+                 precision: int = DNS_PREC_FP64) -> float:
     """J = E(T) of adjoint_energy without its gradient: the forward sweep of
-    dns_adjoint_energy alone (all gradient pointers NULL), same arithmetic,
-    so J is the value adjoint_energy returns."""
+    dns_adjoint_energy_prec alone (all gradient pointers NULL), same
+    arithmetic, so J is the value adjoint_energy returns."""
     lib = load_library()
     U, V, W = _f64(U), _f64(V), _f64(W)
     n = round(U.size ** (1.0 / 3))
     J = ctypes.c_double()
-    _check(lib.dns_adjoint_energy(n, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, 1,
-                                  ctypes.byref(J), None, None, None, None))
+    _check(lib.dns_adjoint_energy_prec(n, precision, _ptr(U), _ptr(V), _ptr(W), nu, dt, nsteps, 1,
+                                       ctypes.byref(J), None, None, None, None))
     return J.value
 
 

@@ -1,5 +1,7 @@
-// adjoint.cuh -- pointwise kernels of the discrete adjoint of the RK4 step
-// (FP64).  The forward stage of main.c:344-413 is, per RK stage s with input
+// adjoint.cuh -- pointwise kernels of the discrete adjoint of the RK4 step.
+// Templates on the storage complex type C (double2 for the FP64 adjoint,
+// float2 for the mixed one); the arithmetic is FP64 in registers, rounded
+// once on store.  The forward stage of main.c:344-413 is, per RK stage s with input
 // U_s (half spectrum) and, at s == 0, the stale real velocity:
 //   u   = s > 0 ? a c2r(U_s) : stale          a = 1/n^3
 //   w   = a c2r(D U_s)                        D U = i k x U  (curl)
@@ -58,23 +60,25 @@ __device__ __forceinline__ void curl_at(const PointK &p, cd u, cd v, cd w, cd &o
 }
 
 // out = curl(in) on 3 slots
-__global__ void k_curl(const cd *__restrict__ in, cd *__restrict__ out, Geo g) {
+template <class C>
+__global__ void k_curl(const C *__restrict__ in, C *__restrict__ out, Geo g) {
   DNSB_FOR_POINTS(g) {
     const PointK p = point_k(g, q);
     cd ox, oy, oz;
-    curl_at(p, in[p.o], in[g.slot + p.o], in[2 * g.slot + p.o], ox, oy, oz);
-    out[p.o] = ox;
-    out[g.slot + p.o] = oy;
-    out[2 * g.slot + p.o] = oz;
+    curl_at(p, to_d(in[p.o]), to_d(in[g.slot + p.o]), to_d(in[2 * g.slot + p.o]), ox, oy, oz);
+    out[p.o] = from_d<C>(ox);
+    out[g.slot + p.o] = from_d<C>(oy);
+    out[2 * g.slot + p.o] = from_d<C>(oz);
   }
 }
 
 // out = (m dt Pi(ldU)) / w_z : the adjoint of N_hat, divided by the c2r
 // weights so that a plain c2r of `out` is r2c^T of m dt Pi(ldU)
-__global__ void k_adj_lamN(const cd *__restrict__ ldU, cd *__restrict__ out, Geo g, double dt) {
+template <class C>
+__global__ void k_adj_lamN(const C *__restrict__ ldU, C *__restrict__ out, Geo g, double dt) {
   DNSB_FOR_POINTS(g) {
     const PointK p = point_k(g, q);
-    cd x = ldU[p.o], y = ldU[g.slot + p.o], z = ldU[2 * g.slot + p.o];
+    cd x = to_d(ldU[p.o]), y = to_d(ldU[g.slot + p.o]), z = to_d(ldU[2 * g.slot + p.o]);
     if (p.kk > 0) {
       const double sr = (x.x * p.kx + y.x * p.ky + z.x * p.kz) / p.kk;
       const double si = (x.y * p.kx + y.y * p.ky + z.y * p.kz) / p.kk;
@@ -83,16 +87,18 @@ __global__ void k_adj_lamN(const cd *__restrict__ ldU, cd *__restrict__ out, Geo
       z = make_double2(z.x - sr * p.kz, z.y - si * p.kz);
     }
     const double s = (p.in ? dt : 0.0) / p.wz;
-    out[p.o] = cscale(x, s);
-    out[g.slot + p.o] = cscale(y, s);
-    out[2 * g.slot + p.o] = cscale(z, s);
+    out[p.o] = from_d<C>(cscale(x, s));
+    out[g.slot + p.o] = from_d<C>(cscale(y, s));
+    out[2 * g.slot + p.o] = from_d<C>(cscale(z, s));
   }
 }
 
-// lu = om x lN (+ lstale_out), lom = lN x u   on [3][n^3] real arrays
-__global__ void k_adj_cross(const double *__restrict__ u, const double *__restrict__ om,
+// lu = om x lN (+ lstale_out), lom = lN x u   on [3][n^3] real arrays (u
+// and the outputs in the storage precision, the rest float64)
+template <class RU, class RO>
+__global__ void k_adj_cross(const RU *__restrict__ u, const double *__restrict__ om,
                             const double *__restrict__ lN, const double *__restrict__ lstale_out,
-                            double *__restrict__ lu, double *__restrict__ lom, long long nr) {
+                            RO *__restrict__ lu, RO *__restrict__ lom, long long nr) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nr;
        q += (long long)gridDim.x * blockDim.x) {
     const double ux = u[q], uy = u[nr + q], uz = u[2 * nr + q];
@@ -104,38 +110,38 @@ __global__ void k_adj_cross(const double *__restrict__ u, const double *__restri
       ay += lstale_out[nr + q];
       az += lstale_out[2 * nr + q];
     }
-    lu[q] = ax;
-    lu[nr + q] = ay;
-    lu[2 * nr + q] = az;
-    lom[q] = ly * uz - lz * uy;
-    lom[nr + q] = lz * ux - lx * uz;
-    lom[2 * nr + q] = lx * uy - ly * ux;
+    lu[q] = (RO)ax;
+    lu[nr + q] = (RO)ay;
+    lu[2 * nr + q] = (RO)az;
+    lom[q] = (RO)(ly * uz - lz * uy);
+    lom[nr + q] = (RO)(lz * ux - lx * uz);
+    lom[2 * nr + q] = (RO)(lx * uy - ly * ux);
   }
 }
 
 // lUs = a w_z (curl(Rw) + Ru) - nu dt kk ldU       (Ru may be null: stage 0)
 // and the nu-gradient terms <ldU, -dt kk Us>, double-double block partials
-template <int BS>
+template <int BS, class C>
 __global__ void __launch_bounds__(BS)
-    k_adj_collect(const cd *__restrict__ Rw, const cd *__restrict__ Ru, const cd *__restrict__ ldU,
-                  const cd *__restrict__ Us, cd *__restrict__ out, Geo g, double a, double nu,
+    k_adj_collect(const C *__restrict__ Rw, const C *__restrict__ Ru, const C *__restrict__ ldU,
+                  const C *__restrict__ Us, C *__restrict__ out, Geo g, double a, double nu,
                   double dt, double4 *__restrict__ partial) {
   DD gn{0.0, 0.0}, unused{0.0, 0.0};
   DNSB_FOR_POINTS(g) {
     const PointK p = point_k(g, q);
     cd cx, cy, cz;
-    curl_at(p, Rw[p.o], Rw[g.slot + p.o], Rw[2 * g.slot + p.o], cx, cy, cz);
+    curl_at(p, to_d(Rw[p.o]), to_d(Rw[g.slot + p.o]), to_d(Rw[2 * g.slot + p.o]), cx, cy, cz);
     if (Ru) {
-      cx = cadd(cx, Ru[p.o]);
-      cy = cadd(cy, Ru[g.slot + p.o]);
-      cz = cadd(cz, Ru[2 * g.slot + p.o]);
+      cx = cadd(cx, to_d(Ru[p.o]));
+      cy = cadd(cy, to_d(Ru[g.slot + p.o]));
+      cz = cadd(cz, to_d(Ru[2 * g.slot + p.o]));
     }
     const double s = a * p.wz, c = nu * dt * p.kk;
-    const cd lx = ldU[p.o], ly = ldU[g.slot + p.o], lz = ldU[2 * g.slot + p.o];
-    out[p.o] = make_double2(s * cx.x - c * lx.x, s * cx.y - c * lx.y);
-    out[g.slot + p.o] = make_double2(s * cy.x - c * ly.x, s * cy.y - c * ly.y);
-    out[2 * g.slot + p.o] = make_double2(s * cz.x - c * lz.x, s * cz.y - c * lz.y);
-    const cd ux = Us[p.o], uy = Us[g.slot + p.o], uz = Us[2 * g.slot + p.o];
+    const cd lx = to_d(ldU[p.o]), ly = to_d(ldU[g.slot + p.o]), lz = to_d(ldU[2 * g.slot + p.o]);
+    out[p.o] = from_d<C>(make_double2(s * cx.x - c * lx.x, s * cx.y - c * lx.y));
+    out[g.slot + p.o] = from_d<C>(make_double2(s * cy.x - c * ly.x, s * cy.y - c * ly.y));
+    out[2 * g.slot + p.o] = from_d<C>(make_double2(s * cz.x - c * lz.x, s * cz.y - c * lz.y));
+    const cd ux = to_d(Us[p.o]), uy = to_d(Us[g.slot + p.o]), uz = to_d(Us[2 * g.slot + p.o]);
     const double dotp = lx.x * ux.x + lx.y * ux.y + ly.x * uy.x + ly.y * uy.y + lz.x * uz.x +
                         lz.y * uz.y;
     gn = dd_add_d(gn, -dt * p.kk * dotp);
@@ -160,27 +166,30 @@ __global__ void __launch_bounds__(BS) k_dd_accumulate(const double4 *__restrict_
 }
 
 // out = a x + b y on 3 slots (y may be null)
-__global__ void k_lincomb3(const cd *__restrict__ x, const cd *__restrict__ y, cd *__restrict__ out,
+template <class C>
+__global__ void k_lincomb3(const C *__restrict__ x, const C *__restrict__ y, C *__restrict__ out,
                            Geo g, double a, double b) {
   DNSB_FOR_POINTS(g) {
     const long long row = q / g.nf;
     const long long o = row * g.nfp + (q - row * g.nf);
 #pragma unroll
     for (int f = 0; f < 3; f++) {
-      const cd xv = x[f * g.slot + o];
+      const cd xv = to_d(x[f * g.slot + o]);
       cd r = cscale(xv, a);
-      if (y) r = cadd(r, cscale(y[f * g.slot + o], b));
-      out[f * g.slot + o] = r;
+      if (y) r = cadd(r, cscale(to_d(y[f * g.slot + o]), b));
+      out[f * g.slot + o] = from_d<C>(r);
     }
   }
 }
 
 // out = x / w_z on 3 slots (r2c^T = c2r of this)
-__global__ void k_div_wz3(const cd *__restrict__ x, cd *__restrict__ out, Geo g) {
+template <class C>
+__global__ void k_div_wz3(const C *__restrict__ x, C *__restrict__ out, Geo g) {
   DNSB_FOR_POINTS(g) {
     const PointK p = point_k(g, q);
 #pragma unroll
-    for (int f = 0; f < 3; f++) out[f * g.slot + p.o] = cscale(x[f * g.slot + p.o], 1.0 / p.wz);
+    for (int f = 0; f < 3; f++)
+      out[f * g.slot + p.o] = from_d<C>(cscale(to_d(x[f * g.slot + p.o]), 1.0 / p.wz));
   }
 }
 

@@ -859,7 +859,8 @@ int set_coef(const Group &G, cudaStream_t st, const double *nu, const double *dt
 
 
 // ---------------------------------------------------------------------------
-// Discrete adjoint of the RK4 step (FP64): gradient of the final energy
+// Discrete adjoint of the RK4 step (FP64, or with the mixed path's FP32
+// storage and transforms): gradient of the final energy
 // E(T) = invn3^2 sum_half |U_hat(T)|^2 (main.c:257-266's definition) with
 // respect to the initial velocity and nu.  Checkpoints of the step state
 // (U_hat, stale velocity) follow a binomial split of the step range.
@@ -876,22 +877,28 @@ struct Adj {
   cudaStream_t st = nullptr;
   cudaGraphExec_t graph = nullptr;
   char *arena = nullptr;
-  cd *sp = nullptr;        // [NX][slot]
-  double *re = nullptr;    // [NRE][n^3]
-  cd *snap_sp = nullptr;   // [S][3][slot]
-  double *snap_re = nullptr;  // [S][3][n^3]
+  void *sp = nullptr;        // [NX][slot], storage complex type
+  double *re = nullptr;      // [NRE][n^3] float64; LU, LOM, STALEIN hold the storage real type
+  char *snap_sp = nullptr;   // [S][3][slot]
+  char *snap_re = nullptr;   // [S][3][n^3], storage real type
   double4 *part = nullptr, *acc_nu = nullptr;
   int nblocks = 0;
   double nu = 0, dt = 0;
-  cd *X(int i) const { return sp + (size_t)i * G.g.slot; }
+  template <class C>
+  C *X(int i) const { return (C *)sp + (size_t)i * G.g.slot; }
   double *Rf(int i) const { return re + (size_t)i * G.g.nreal; }
-  size_t slot3() const { return (size_t)3 * G.g.slot * sizeof(cd); }
-  size_t real3() const { return (size_t)3 * G.g.nreal * sizeof(double); }
+  // a real triple seen in the storage type (3 n^3 values fit in its space)
+  template <class R>
+  R *Rr(int i) const { return (R *)(re + (size_t)i * G.g.nreal); }
+  size_t slot3() const { return (size_t)3 * G.g.slot * G.csize; }
+  size_t real3() const { return (size_t)3 * G.g.nreal * G.rsize; }
+  size_t real3d() const { return (size_t)3 * G.g.nreal * sizeof(double); }
 };
 
-template <int N>
+template <class R, int N>
 struct AdjOps {
-  using O = Ops<double, N>;
+  using O = Ops<R, N>;
+  using C = cx<R>;
   static int copy3(Adj &A, void *dst, const void *src, size_t bytes) {
     CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, A.st));
     return DNS_OK;
@@ -905,29 +912,30 @@ struct AdjOps {
     const Geo &g = G.g;
     const double a = 1.0 / (double)g.nreal;
     const int t3[3] = {0, 1, 2};
-    const cd *Us = A.X(X_US0 + 3 * s);
-    const double *u = A.Rf(RE_STALEIN);
-    if (s > 0) {
-      O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
-      u = A.Rf(RE_U);
-    }
+    const C *Us = A.X<C>(X_US0 + 3 * s);
+    if (s > 0) O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
     const unsigned pb = pblocks(A);
-    k_curl<<<pb, 256, 0, A.st>>>(Us, A.X(X_T1), g);
-    O::c2r_fields(G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_OM), a);
-    k_adj_lamN<<<pb, 256, 0, A.st>>>(A.X(X_LDU), A.X(X_T1), g, A.dt);
-    O::c2r_fields(G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
-    k_adj_cross<<<conv_blocks(g.nreal), 256, 0, A.st>>>(
-        u, A.Rf(RE_OM), A.Rf(RE_LN), s == 3 ? A.Rf(RE_LSTALE) : nullptr, A.Rf(RE_LU),
-        A.Rf(RE_LOM), g.nreal);
-    O::r2c_fields(G, A.st, A.Rf(RE_LOM), 3, A.X(X_T1), t3);
-    if (s > 0) O::r2c_fields(G, A.st, A.Rf(RE_LU), 3, A.X(X_T2), t3);
-    k_adj_collect<256><<<pb, 256, 0, A.st>>>(A.X(X_T1), s > 0 ? A.X(X_T2) : nullptr, A.X(X_LDU), Us,
-                                             A.X(X_LUS), g, a, A.nu, A.dt, A.part);
+    k_curl<C><<<pb, 256, 0, A.st>>>(Us, A.X<C>(X_T1), g);
+    O::c2r_fields(G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_OM), a);
+    k_adj_lamN<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LDU), A.X<C>(X_T1), g, A.dt);
+    O::c2r_fields(G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
+    if (s > 0)
+      k_adj_cross<double, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
+          A.Rf(RE_U), A.Rf(RE_OM), A.Rf(RE_LN), s == 3 ? A.Rf(RE_LSTALE) : nullptr,
+          A.Rr<R>(RE_LU), A.Rr<R>(RE_LOM), g.nreal);
+    else  // stage 0 reads the stale velocity (main.c:344)
+      k_adj_cross<R, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
+          A.Rr<R>(RE_STALEIN), A.Rf(RE_OM), A.Rf(RE_LN), nullptr, A.Rr<R>(RE_LU),
+          A.Rr<R>(RE_LOM), g.nreal);
+    O::r2c_fields(G, A.st, A.Rr<R>(RE_LOM), 3, A.X<C>(X_T1), t3);
+    if (s > 0) O::r2c_fields(G, A.st, A.Rr<R>(RE_LU), 3, A.X<C>(X_T2), t3);
+    k_adj_collect<256, C><<<pb, 256, 0, A.st>>>(A.X<C>(X_T1), s > 0 ? A.X<C>(X_T2) : nullptr,
+                                                A.X<C>(X_LDU), Us, A.X<C>(X_LUS), g, a, A.nu, A.dt,
+                                                A.part);
     k_dd_accumulate<256><<<1, 256, 0, A.st>>>(A.part, A.nblocks, A.acc_nu);
-    if (s == 0) {
-      int r = copy3(A, A.Rf(RE_LSTALE), A.Rf(RE_LU), A.real3());
-      if (r != DNS_OK) return r;
-    }
+    if (s == 0)  // lambda of the step's input stale velocity, kept in float64
+      k_real_convert<R, double><<<conv_blocks(3 * g.nreal), 256, 0, A.st>>>(
+          A.Rr<R>(RE_LU), A.Rf(RE_LSTALE), 3 * g.nreal);
     CKL();
     return DNS_OK;
   }
@@ -939,41 +947,43 @@ struct AdjOps {
     const Geo &g = G.g;
     const unsigned pb = pblocks(A);
     int r;
-    if ((r = copy3(A, A.X(X_US0), G.slot_ptr(0, SLOT_SA), A.slot3()))) return r;
-    if ((r = copy3(A, A.Rf(RE_STALEIN), G.stale, A.real3()))) return r;
+    if ((r = copy3(A, A.X<C>(X_US0), G.slot_ptr(0, SLOT_SA), A.slot3()))) return r;
+    if ((r = copy3(A, A.Rr<R>(RE_STALEIN), G.stale, A.real3()))) return r;
     for (int s = 0; s < 4; s++) {  // forward again, keeping the stage inputs
       for (int k = 0; k < KERNELS_PER_STAGE; k++) O::stage_kernel(G, A.st, s, k);
-      if (s < 3 && (r = copy3(A, A.X(X_US0 + 3 * (s + 1)), G.slot_ptr(0, SLOT_SB), A.slot3())))
+      if (s < 3 && (r = copy3(A, A.X<C>(X_US0 + 3 * (s + 1)), G.slot_ptr(0, SLOT_SB), A.slot3())))
         return r;
     }
-    if ((r = copy3(A, A.X(X_LACC), A.X(X_LHAT), A.slot3()))) return r;
-    if ((r = copy3(A, A.X(X_LHAT0), A.X(X_LHAT), A.slot3()))) return r;  // acc_0 = U0
+    if ((r = copy3(A, A.X<C>(X_LACC), A.X<C>(X_LHAT), A.slot3()))) return r;
+    if ((r = copy3(A, A.X<C>(X_LHAT0), A.X<C>(X_LHAT), A.slot3()))) return r;  // acc_0 = U0
     for (int s = 3; s >= 0; s--) {
       if (s == 3)
-        k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LACC), nullptr, A.X(X_LDU), g, RK_A[3], 0.0);
+        k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LACC), nullptr, A.X<C>(X_LDU), g, RK_A[3], 0.0);
       else  // U_{s+1} = U0 + b_s dU_s, acc += a_s dU_s
-        k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LUS), A.X(X_LACC), A.X(X_LDU), g, RK_B[s], RK_A[s]);
+        k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LUS), A.X<C>(X_LACC), A.X<C>(X_LDU), g,
+                                            RK_B[s], RK_A[s]);
       if ((r = stage(A, s))) return r;
       // every stage input U_s is U0 plus a multiple of dU_{s-1}
-      k_lincomb3<<<pb, 256, 0, A.st>>>(A.X(X_LHAT0), A.X(X_LUS), A.X(X_LHAT0), g, 1.0, 1.0);
+      k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LHAT0), A.X<C>(X_LUS), A.X<C>(X_LHAT0), g, 1.0,
+                                          1.0);
     }
-    if ((r = copy3(A, A.X(X_LHAT), A.X(X_LHAT0), A.slot3()))) return r;
+    if ((r = copy3(A, A.X<C>(X_LHAT), A.X<C>(X_LHAT0), A.slot3()))) return r;
     CKL();
     return DNS_OK;
   }
 };
 
 int adj_snap_store(Adj &A, int k) {
-  CK(cudaMemcpyAsync(A.snap_sp + (size_t)k * 3 * A.G.g.slot, A.G.slot_ptr(0, SLOT_SA), A.slot3(),
+  CK(cudaMemcpyAsync(A.snap_sp + (size_t)k * A.slot3(), A.G.slot_ptr(0, SLOT_SA), A.slot3(),
                      cudaMemcpyDeviceToDevice, A.st));
-  CK(cudaMemcpyAsync(A.snap_re + (size_t)k * 3 * A.G.g.nreal, A.G.stale, A.real3(),
+  CK(cudaMemcpyAsync(A.snap_re + (size_t)k * A.real3(), A.G.stale, A.real3(),
                      cudaMemcpyDeviceToDevice, A.st));
   return DNS_OK;
 }
 int adj_snap_restore(Adj &A, int k) {
-  CK(cudaMemcpyAsync(A.G.slot_ptr(0, SLOT_SA), A.snap_sp + (size_t)k * 3 * A.G.g.slot, A.slot3(),
+  CK(cudaMemcpyAsync(A.G.slot_ptr(0, SLOT_SA), A.snap_sp + (size_t)k * A.slot3(), A.slot3(),
                      cudaMemcpyDeviceToDevice, A.st));
-  CK(cudaMemcpyAsync(A.G.stale, A.snap_re + (size_t)k * 3 * A.G.g.nreal, A.real3(),
+  CK(cudaMemcpyAsync(A.G.stale, A.snap_re + (size_t)k * A.real3(), A.real3(),
                      cudaMemcpyDeviceToDevice, A.st));
   return DNS_OK;
 }
@@ -985,7 +995,7 @@ int adj_step_one(Adj &A) {
   int r = DNS_OK;
   dispatch(A.G, [&](auto ops) {
     using O = decltype(ops);
-    r = AdjOps<O::Nval>::step(A);
+    r = AdjOps<typename O::Real, O::Nval>::step(A);
   });
   return r;
 }
@@ -1664,14 +1674,16 @@ int dns_ens_synchronize(dns_ens *e) {
 /* discrete adjoint                                                    */
 /* ------------------------------------------------------------------ */
 
-int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
-                       double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
-                       double *gW, double *gnu) {
+int dns_adjoint_energy_prec(long n, int precision, const double *U, const double *V,
+                            const double *W, double nu, double dt, long nsteps, int snapshots,
+                            double *J, double *gU, double *gV, double *gW, double *gnu) {
   if (!U || !V || !W || nsteps < 1 || snapshots < 1)
     return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
+  if (precision != DNS_PREC_FP64 && precision != DNS_PREC_MIXED)
+    return fail(DNS_ERR_ARG, "unknown precision", __FILE__, __LINE__);
   Adj A;
   CK(cudaStreamCreateWithFlags(&A.st, cudaStreamNonBlocking));
-  int r = group_init(A.G, n, DNS_PREC_FP64, 0, 1, A.st);
+  int r = group_init(A.G, n, precision, 0, 1, A.st);
   auto cleanup = [&]() {
     if (A.st) cudaStreamSynchronize(A.st);
     if (A.graph) cudaGraphExecDestroy(A.graph);
@@ -1685,10 +1697,10 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
   A.dt = dt;
   A.nblocks = A.G.diag_blocks;
   if (r == DNS_OK) {
-    const size_t sp_b = (size_t)NX * g.slot * sizeof(cd);
+    const size_t sp_b = (size_t)NX * g.slot * A.G.csize;
     const size_t re_b = (size_t)NRE * g.nreal * sizeof(double);
-    const size_t ssp_b = (size_t)snapshots * 3 * g.slot * sizeof(cd);
-    const size_t sre_b = (size_t)snapshots * 3 * g.nreal * sizeof(double);
+    const size_t ssp_b = (size_t)snapshots * A.slot3();
+    const size_t sre_b = (size_t)snapshots * A.real3();
     const size_t part_b = (size_t)(A.nblocks + 1) * sizeof(double4);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     cudaError_t e = cudaMalloc((void **)&A.arena, al(sp_b) + al(re_b) + al(ssp_b) + al(sre_b) + al(part_b));
@@ -1697,10 +1709,10 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
       r = fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
     } else {
       char *p = A.arena;
-      A.sp = (cd *)p; p += al(sp_b);
+      A.sp = p; p += al(sp_b);
       A.re = (double *)p; p += al(re_b);
-      A.snap_sp = (cd *)p; p += al(ssp_b);
-      A.snap_re = (double *)p; p += al(sre_b);
+      A.snap_sp = p; p += al(ssp_b);
+      A.snap_re = p; p += al(sre_b);
       A.part = (double4 *)p;
       A.acc_nu = A.part + A.nblocks;
       e = cudaMemsetAsync(A.arena, 0, al(sp_b) + al(re_b), A.st);
@@ -1743,19 +1755,23 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
   if (r == DNS_OK) {
     // lambda(T) = dE/dU_hat = 2 invn3^2 U_hat(T); the stale velocity at T
     // does not enter E
-    k_lincomb3<<<A.nblocks, 256, 0, A.st>>>((const cd *)A.G.slot_ptr(0, SLOT_SA), nullptr,
-                                            A.X(X_LHAT), g, 2.0 * invn3 * invn3, 0.0);
-    cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3(), A.st);
+    dispatch(A.G, [&](auto ops) {
+      using C = typename decltype(ops)::C;
+      k_lincomb3<C><<<A.nblocks, 256, 0, A.st>>>((const C *)A.G.slot_ptr(0, SLOT_SA), nullptr,
+                                                 A.X<C>(X_LHAT), g, 2.0 * invn3 * invn3, 0.0);
+    });
+    cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3d(), A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
   if (r == DNS_OK) r = adj_reverse(A, 0, nsteps, 0, snapshots - 1);
   if (r == DNS_OK) {
     // dE/du0 = r2c^T(lambda_U(0)) + lambda_stale(0) = c2r(lambda / w_z) + lambda_stale
     const int t3[3] = {0, 1, 2};
-    k_div_wz3<<<A.nblocks, 256, 0, A.st>>>(A.X(X_LHAT), A.X(X_T1), g);
     dispatch(A.G, [&](auto ops) {
       using O = decltype(ops);
-      Ops<double, O::Nval>::c2r_fields(A.G, A.st, A.X(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
+      using C = typename O::C;
+      k_div_wz3<C><<<A.nblocks, 256, 0, A.st>>>(A.X<C>(X_LHAT), A.X<C>(X_T1), g);
+      O::c2r_fields(A.G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
     });
     k_add_real<<<conv_blocks(3 * g.nreal), 256, 0, A.st>>>(A.Rf(RE_LSTALE), A.Rf(RE_LN), 3 * g.nreal);
     cudaError_t e = cudaGetLastError();
@@ -1773,6 +1789,13 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
   }
   cleanup();
   return r;
+}
+
+int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
+                       double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
+                       double *gW, double *gnu) {
+  return dns_adjoint_energy_prec(n, DNS_PREC_FP64, U, V, W, nu, dt, nsteps, snapshots, J, gU, gV,
+                                 gW, gnu);
 }
 
 }  // extern "C"

@@ -229,6 +229,17 @@ int dns_ens_synchronize(dns_ens *e);
 int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
                        double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
                        double *gW, double *gnu);
+/* The same with a choice of precision: DNS_PREC_FP64 (dns_adjoint_energy)
+ * or DNS_PREC_MIXED, whose forward recomputation is the mixed step itself
+ * (FP32 spectral storage and transforms, FP64 viscous coefficients and
+ * reductions) and whose transposed step keeps the same FP32 storage and
+ * transforms with its pointwise products, the nu gradient and the float64
+ * host-facing gradient in FP64.  Its J is the mixed path's E(T), its
+ * gradient the exact adjoint of that rounded map to within FP32 transform
+ * error (about 1e-5 relative to the FP64 gradient). */
+int dns_adjoint_energy_prec(long n, int precision, const double *U, const double *V,
+                            const double *W, double nu, double dt, long nsteps, int snapshots,
+                            double *J, double *gU, double *gV, double *gW, double *gnu);
 
 /* Energy and enstrophy of a spectral velocity held in caller-owned device
  * memory, allocating nothing.  No counterpart in the reference (main.c has

@@ -99,3 +99,60 @@ def test_adjoint_config(dns, n):
     J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20)
     dirs = [dns.solenoidal_perturbation(n, seed=k) for k in range(1, 9)]
     fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, dirs)
+
+
+def _rel(a, b):
+    return float(np.sqrt(sum(np.sum((a[c] - b[c]) ** 2) for c in range(3)) /
+                         sum(np.sum(b[c] ** 2) for c in range(3))))
+
+
+def test_mixed_adjoint_against_fp64_adjoint(dns):
+    """The mixed-precision adjoint (FP32 storage and transforms) against the
+    FP64 adjoint, itself pinned to finite differences above: J equals the
+    mixed forward run's energy exactly, and J, the velocity gradient (L2 over
+    all points) and the nu gradient agree with FP64 to 1e-4 relative (FP32
+    transform error, ~1e-6 per transform, accumulated over the steps)."""
+    n, nu, dt, nsteps = 32, 0.02, 0.01, 12
+    u0 = dns.perturbed_tgv(n, seed=5, amplitude=0.3)
+    J64, g64, gnu64 = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=4)
+    J32, g32, gnu32 = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=4,
+                                         precision=dns.DNS_PREC_MIXED)
+    with dns.Context(n, dns.DNS_PREC_MIXED) as ctx:
+        ctx.set_velocity(*u0)
+        ctx.step(nu, dt, nsteps)
+        E, _ = ctx.diagnostics()
+    assert J32 == pytest.approx(float(E), rel=1e-14)
+    assert J32 == dns.final_energy(*u0, nu, dt, nsteps, precision=dns.DNS_PREC_MIXED)
+    eg, enu = _rel(g32, g64), abs(gnu32 - gnu64) / abs(gnu64)
+    print(f"\nmixed vs FP64 adjoint, n={n} steps={nsteps}: J rel {abs(J32 - J64) / J64:.2e}, "
+          f"gradient rel L2 {eg:.2e}, nu gradient rel {enu:.2e}")
+    assert abs(J32 - J64) <= 1e-4 * J64
+    assert eg <= 1e-4 and enu <= 1e-4
+    # checkpointing leaves the mixed gradient bit-identical too
+    J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=1,
+                                   precision=dns.DNS_PREC_MIXED)
+    assert J == J32 and gnu == gnu32
+    for c in range(3):
+        assert np.array_equal(g[c], g32[c])
+
+
+def test_mixed_adjoint_config_128(dns):
+    """The adjoint configuration (random isotropic field of unit energy,
+    128^3, nu = dt = 0.005, 401 steps, 20 snapshots) in mixed precision
+    against FP64: gradient rel L2 and nu gradient within 1e-3 (the 401-step
+    mixed forward itself differs from FP64 by ~1e-5 in energy)."""
+    n, nu, dt = 128, 0.005, 0.005
+    _, nsteps = dns.step_schedule(2.0, dt)
+    u0 = dns.solenoidal_perturbation(n, seed=0)
+    with dns.Context(n) as ctx:
+        ctx.set_velocity(*u0)
+        E0, _ = ctx.diagnostics()
+    u0 = [c * float(1.0 / np.sqrt(E0)) for c in u0]
+    J64, g64, gnu64 = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20)
+    J32, g32, gnu32 = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20,
+                                         precision=dns.DNS_PREC_MIXED)
+    eg, enu = _rel(g32, g64), abs(gnu32 - gnu64) / abs(gnu64)
+    print(f"\nmixed vs FP64 adjoint, n={n} steps={nsteps}: J rel {abs(J32 - J64) / J64:.2e}, "
+          f"gradient rel L2 {eg:.2e}, nu gradient rel {enu:.2e}")
+    assert abs(J32 - J64) <= 1e-4 * J64
+    assert eg <= 1e-3 and enu <= 1e-3
