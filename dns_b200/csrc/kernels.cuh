@@ -686,8 +686,6 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       // place and leave.  The last stage stores the velocity as the next
       // stale one as it comes.
       R su[Z::S2 ? 1 : E], soy[Z::S2 ? 1 : E];  // FP32: (u, omega_y) in registers
-      auto U_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(0, e); else return su[e]; };
-      auto OY_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(1, e); else return soy[e]; };
       ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
         const C uu = ld(pU, s), d = ld(pDWDX, s);
         a = uu;
@@ -708,6 +706,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
         }
         if (KIND == 2 && ok) stale[roff + t + T * e] = u;
       }
+      auto U_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(0, e); else return su[e]; };
+      auto OY_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(1, e); else return soy[e]; };
       ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
         const C vv = ld(pV, s), d = ld(pDWDY, s);
         a = vv;
