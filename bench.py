@@ -295,6 +295,9 @@ def ensemble_leg(steps: int, warmup: int):
         eo.synchronize()
         other = {"schedule": "persistent" if chosen == "batched" else "batched",
                  "ms_per_ensemble_step": oms, "value": len(sizes) / (oms / 1000.0)}
+    # the sequential arm does the ensemble's work (every run of a size steps
+    # `steps` times, one after another), so that it runs as long, under the
+    # same power cap, as the ensemble
     seq_ms = {}
     for n in (64, 128):
         with dns_b200.Context(n, prec) as c:
@@ -305,11 +308,12 @@ def ensemble_leg(steps: int, warmup: int):
             c.synchronize()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
+            nseq = sizes.count(n) * steps
             a.record(sc)
-            c.step(float(nus[r]), dt, steps)
+            c.step(float(nus[r]), dt, nseq)
             b.record(sc)
             b.synchronize()
-            seq_ms[n] = a.elapsed_time(b) / steps
+            seq_ms[n] = a.elapsed_time(b) / nseq
     agg = len(sizes) * steps / (ms / 1000.0)
     seq = len(sizes) / ((32 * seq_ms[64] + 16 * seq_ms[128]) / 1000.0)
     peak, peak_kind = load_peak()

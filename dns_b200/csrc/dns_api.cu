@@ -26,6 +26,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <type_traits>
 #include <string>
@@ -113,6 +114,10 @@ struct Group {
   double *coef = nullptr;        // [nruns][2]: nu, dt
   int diag_blocks = 0;
   double *realbuf = nullptr;     // [4][n^3] float64, allocated on first field read
+  // column-pass register schedules [axis][forward] picked by the autotuner
+  // for this group's launches, and the run count they were timed on
+  int pick[2][2] = {{0, 0}, {0, 0}};
+  int tune_runs = 1;
 
   char *slot_ptr(int run, int s) const {
     return (char *)S + ((size_t)run * g.run_spec + (size_t)s * g.slot) * csize;
@@ -224,8 +229,9 @@ struct Ops {
   // kernel compiled with a minimum of ColCands::m[I] resident blocks per SM
   // (0: the compiler's own register choice); the candidates differ only in
   // register allocation, so every one computes bit-identical results.  The
-  // autotuner (tune()) times them once per process and size and keeps the
-  // fastest; sizes below 64 have the compiler's choice only.
+  // autotuner (tune()) times them once per process, size and batch shape
+  // (the run count it times on) and keeps the fastest; sizes below 64 have
+  // the compiler's choice only.
   using ColFn = void (*)(const C *, C *, const C *, Geo, ColJobs);
   template <int AXIS>
   using Cands = ColCands<(N >= 64 ? (N / Plan<N>::E) * ColW<R, AXIS, N>::W : 0), (int)sizeof(C)>;
@@ -244,13 +250,23 @@ struct Ops {
     }
     return col_cand<AXIS, FWD, I>();
   }
-  // chosen candidate of [AXIS][FWD] and its measured time per launch (ms)
-  static inline int col_pick[2][2] = {{0, 0}, {0, 0}};
-  static inline float col_ms[2][2][16] = {};
-  static inline bool tuned = false;
+  // chosen candidate of [AXIS][FWD] and the measured time per launch (ms)
+  // of every candidate, per tuning run count
+  struct TuneRec {
+    int pick[2][2];
+    float ms[2][2][16];
+  };
+  static inline std::map<int, TuneRec> tune_cache;
   template <int AXIS, bool FWD>
-  static ColFn colkern() {
-    return col_cand_at<AXIS, FWD>(col_pick[AXIS][FWD]);
+  static ColFn colkern(const Group &G) {
+    return col_cand_at<AXIS, FWD>(G.pick[AXIS][FWD]);
+  }
+  // runs a batch is tuned on: all of them up to the volume of two 256^3
+  // runs, which fills the GPU like any larger batch
+  static int tune_runs(int nruns) {
+    long long cap = 2LL * 256 * 256 * 256 / ((long long)N * N * N);
+    if (cap < 1) cap = 1;
+    return (int)(nruns < cap ? nruns : cap);
   }
 
   template <class K>
@@ -280,22 +296,24 @@ struct Ops {
 
   // ---- autotuner of the column-pass register schedules ----
   template <int AXIS, bool FWD>
-  static cudaError_t time_cands(const Group &G1, cudaStream_t st, const ColJobs &jobs,
-                                cudaEvent_t e0, cudaEvent_t e1, int force, int force_m) {
+  static cudaError_t time_cands(Group &Gt, cudaStream_t st, const ColJobs &jobs, cudaEvent_t e0,
+                                cudaEvent_t e1, int force, int force_m, TuneRec &rec) {
     constexpr int n = Cands<AXIS>::n;
+    int &pick = Gt.pick[AXIS][FWD];
     if (force_m >= 0) {  // a given register schedule: its candidate, else the compiler's
-      col_pick[AXIS][FWD] = 0;
+      pick = 0;
       for (int i = 0; i < n; i++)
-        if (Cands<AXIS>::m[i] == force_m) col_pick[AXIS][FWD] = i;
+        if (Cands<AXIS>::m[i] == force_m) pick = i;
+      rec.pick[AXIS][FWD] = pick;
       return cudaSuccess;
     }
     int best = 0;
     for (int i = 0; i < n; i++) {
-      col_pick[AXIS][FWD] = i;
-      colpass_io<AXIS, FWD>(G1, st, (C *)G1.S, (C *)G1.S, jobs, 1);  // warm-up
+      pick = i;
+      colpass_io<AXIS, FWD>(Gt, st, (C *)Gt.S, (C *)Gt.S, jobs, Gt.nruns);  // warm-up
       cudaError_t e = cudaEventRecord(e0, st);
       for (int r = 0; r < 3 && e == cudaSuccess; r++) {
-        colpass_io<AXIS, FWD>(G1, st, (C *)G1.S, (C *)G1.S, jobs, 1);
+        colpass_io<AXIS, FWD>(Gt, st, (C *)Gt.S, (C *)Gt.S, jobs, Gt.nruns);
         e = cudaGetLastError();
       }
       if (e == cudaSuccess) e = cudaEventRecord(e1, st);
@@ -303,29 +321,38 @@ struct Ops {
       float ms = 0.f;
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
       if (e != cudaSuccess) return e;
-      col_ms[AXIS][FWD][i] = ms / 3.f;
-      if (col_ms[AXIS][FWD][i] < col_ms[AXIS][FWD][best]) best = i;
+      rec.ms[AXIS][FWD][i] = ms / 3.f;
+      if (rec.ms[AXIS][FWD][i] < rec.ms[AXIS][FWD][best]) best = i;
     }
-    col_pick[AXIS][FWD] = force >= 0 ? (force < n ? force : n - 1) : best;
+    pick = force >= 0 ? (force < n ? force : n - 1) : best;
+    rec.pick[AXIS][FWD] = pick;
     return cudaSuccess;
   }
   // Time every register schedule of the four column passes of an RK stage
-  // (their real job tables, on the work slots of run 0, whose contents do
-  // not matter to an FFT's timing) and keep the fastest of each; once per
-  // process and size.  DNS_B200_TUNE=0 keeps the compiler's schedule,
+  // (their real job tables, batched over the group's first tune_runs(nruns)
+  // runs, on their work slots, whose contents do not matter to an FFT's
+  // timing) and keep the fastest of each; once per process, size and tuning
+  // run count.  The group launches with the picks (G.pick).  DNS_B200_TUNE=0 keeps the compiler's schedule,
   // DNS_B200_TUNE=f<k> forces candidate k (the last where there are fewer),
   // DNS_B200_TUNE=m<a>,<b>,<c>,<d> the schedules of min blocks/SM a, b, c, d
   // for the x inverse, x forward, y inverse and y forward passes (as
   // dns_get_schedule reports them; a value that is not a candidate means
   // the compiler's).
-  static cudaError_t tune(const Group &G, cudaStream_t st, bool *ran) {
+  static cudaError_t tune(Group &G, cudaStream_t st, bool *ran) {
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     *ran = false;
-    if (tuned) return cudaSuccess;
+    G.tune_runs = tune_runs(G.nruns);
+    auto it = tune_cache.find(G.tune_runs);
+    if (it != tune_cache.end()) {
+      memcpy(G.pick, it->second.pick, sizeof G.pick);
+      return cudaSuccess;
+    }
+    TuneRec rec{};
     const char *env = getenv("DNS_B200_TUNE");
     if (env && strcmp(env, "0") == 0) {
-      tuned = true;
+      tune_cache[G.tune_runs] = rec;
+      memset(G.pick, 0, sizeof G.pick);
       return cudaSuccess;
     }
     const int force = (env && env[0] == 'f') ? atoi(env + 1) : -1;
@@ -338,7 +365,8 @@ struct Ops {
         if (*c == ',') c++;
       }
     }
-    const Group G1 = G.one(0);
+    Group Gt = G;  // the first tune_runs runs
+    Gt.nruns = G.tune_runs;
     const int io[3] = {SLOT_WORK + SNX, SLOT_WORK + SNY, SLOT_WORK + SNZ};
     ColJobs jm = jobs_map(io, io, 3);
     jm.masked = 1;
@@ -346,31 +374,40 @@ struct Ops {
     cudaError_t e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e == cudaSuccess)
-      e = time_cands<0, false>(G1, st, jobs_pass_a(SLOT_WORK), e0, e1, force, fm[0]);
-    if (e == cudaSuccess) e = time_cands<1, false>(G1, st, jobs_pass_b(false), e0, e1, force, fm[2]);
-    if (e == cudaSuccess) e = time_cands<1, true>(G1, st, jm, e0, e1, force, fm[3]);
-    if (e == cudaSuccess) e = time_cands<0, true>(G1, st, jm, e0, e1, force, fm[1]);
+      e = time_cands<0, false>(Gt, st, jobs_pass_a(SLOT_WORK), e0, e1, force, fm[0], rec);
+    if (e == cudaSuccess)
+      e = time_cands<1, false>(Gt, st, jobs_pass_b(false), e0, e1, force, fm[2], rec);
+    if (e == cudaSuccess) e = time_cands<1, true>(Gt, st, jm, e0, e1, force, fm[3], rec);
+    if (e == cudaSuccess) e = time_cands<0, true>(Gt, st, jm, e0, e1, force, fm[1], rec);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    if (e == cudaSuccess) tuned = true;
+    if (e == cudaSuccess) tune_cache[G.tune_runs] = rec;
+    memcpy(G.pick, rec.pick, sizeof G.pick);
     *ran = true;
     return e;
   }
-  // text description of the chosen schedules
-  static std::string schedule() {
+  // text description of the schedules chosen for G
+  static std::string schedule(const Group &G) {
     std::string out;
+    TuneRec rec{};
+    memcpy(rec.pick, G.pick, sizeof rec.pick);
+    {
+      auto it = tune_cache.find(G.tune_runs);
+      if (it != tune_cache.end()) rec = it->second;
+    }
+    if (G.tune_runs > 1) out = "timed on " + std::to_string(G.tune_runs) + " runs: ";
     const char *name[2][2] = {{"x inverse", "x forward"}, {"y inverse", "y forward"}};
     char buf[160];
     for (int a = 0; a < 2; a++)
       for (int f = 0; f < 2; f++) {
         const int n = a == 0 ? Cands<0>::n : Cands<1>::n;
         const int *m = a == 0 ? Cands<0>::m : Cands<1>::m;
-        const int k = col_pick[a][f];
-        snprintf(buf, sizeof buf, "%scolumn pass %s: min blocks/SM %d of {", out.empty() ? "" : "; ",
-                 name[a][f], m[k]);
+        const int k = rec.pick[a][f];
+        snprintf(buf, sizeof buf, "%scolumn pass %s: min blocks/SM %d of {",
+                 (a == 0 && f == 0) ? "" : "; ", name[a][f], m[k]);
         out += buf;
         for (int i = 0; i < n; i++) {
-          snprintf(buf, sizeof buf, "%s%d: %.4f ms", i ? ", " : "", m[i], (double)col_ms[a][f][i]);
+          snprintf(buf, sizeof buf, "%s%d: %.4f ms", i ? ", " : "", m[i], (double)rec.ms[a][f][i]);
           out += buf;
         }
         out += "}";
@@ -395,7 +432,7 @@ struct Ops {
     const int tiles = jobs.masked ? G.g.kcut / CW<AXIS> + 1 : G.g.nfp / CW<AXIS>;
     const int rows = (jobs.masked && AXIS == 0) ? 2 * G.g.kcut + 1 : N;
     dim3 grid(tiles, rows, jobs.njobs * nruns);
-    colkern<AXIS, FWD>()<<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
+    colkern<AXIS, FWD>(G)<<<grid, CT<AXIS>, COL_SMEM<AXIS>, st>>>(in, out, tw(G), G.g, jobs);
   }
   template <int AXIS, bool FWD>
   static void colpass(const Group &G, cudaStream_t st, const ColJobs &jobs) {
@@ -482,8 +519,8 @@ struct Ops {
     const PPhase<R> P = describe(G, s, k);
     const dim3 grid(P.gx, P.gy, P.gz);
     if (P.kind == PK_COL) {
-      ColFn f = P.axis == 0 ? (P.fwd ? colkern<0, true>() : colkern<0, false>())
-                            : (P.fwd ? colkern<1, true>() : colkern<1, false>());
+      ColFn f = P.axis == 0 ? (P.fwd ? colkern<0, true>(G) : colkern<0, false>(G))
+                            : (P.fwd ? colkern<1, true>(G) : colkern<1, false>(G));
       f<<<grid, P.tpi, P.smem, st>>>((C *)G.S, (C *)G.S, tw(G), g, P.jobs);
     } else if (P.kind == PK_Z) {
       if (P.sub == 0)
@@ -702,8 +739,9 @@ int group_init(Group &G, long n, int precision, unsigned flags, int nruns, cudaS
   bool ran = false;
   dispatch(G, [&](auto ops) { te = decltype(ops)::tune(G, st, &ran); });
   CK(te);
-  if (ran) {  // the tuner ran column passes on run 0's work slots: zero them again
-    CK(cudaMemsetAsync(G.slot_ptr(0, SLOT_WORK), 0, (size_t)7 * g.slot * G.csize, st));
+  if (ran) {  // the tuner ran column passes on the work slots of its runs: zero them again
+    for (int r = 0; r < G.tune_runs; r++)
+      CK(cudaMemsetAsync(G.slot_ptr(r, SLOT_WORK), 0, (size_t)7 * g.slot * G.csize, st));
     CK(cudaStreamSynchronize(st));
   }
   return DNS_OK;
@@ -1230,7 +1268,7 @@ int dns_get_info(dns_ctx *c, dns_info_t *info) {
 int dns_get_schedule(dns_ctx *c, char *buf, long len) {
   if (!c || !buf || len < 1) return fail(DNS_ERR_ARG, "bad argument", __FILE__, __LINE__);
   std::string s;
-  dispatch(c->grp, [&](auto ops) { s = decltype(ops)::schedule(); });
+  dispatch(c->grp, [&](auto ops) { s = decltype(ops)::schedule(c->grp); });
   snprintf(buf, (size_t)len, "%s", s.c_str());
   return DNS_OK;
 }
@@ -1598,7 +1636,7 @@ int dns_ens_get_schedule(dns_ens *e, char *buf, long len) {
   s += tmp;
   for (const Group &G : e->groups) {
     std::string g;
-    dispatch(G, [&](auto ops) { g = decltype(ops)::schedule(); });
+    dispatch(G, [&](auto ops) { g = decltype(ops)::schedule(G); });
     snprintf(tmp, sizeof tmp, "; n=%ld: ", G.n);
     s += tmp + g;
   }

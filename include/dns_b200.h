@@ -143,8 +143,10 @@ int dns_get_info(dns_ctx *ctx, dns_info_t *info);
 /* The kernel schedule the library's autotuner chose for this context's grid
  * size and precision (no counterpart in the reference): for each column
  * pass, the register schedule (minimum resident blocks per SM) picked by
- * timing every compiled candidate once per process, with the measured
- * times.  All candidates compute bit-identical results.  The environment
+ * timing every compiled candidate once per process, size, precision and
+ * batch shape, with the measured times (an ensemble group is timed on its
+ * own runs, up to the volume of two 256^3 runs; its schedule then starts
+ * "timed on <k> runs: ").  All candidates compute bit-identical results.  The environment
  * variable DNS_B200_TUNE=0 keeps the compiler's schedule; DNS_B200_TUNE=f<k>
  * forces candidate k; DNS_B200_TUNE=m<a>,<b>,<c>,<d> the schedules of a, b,
  * c, d min blocks/SM for the x inverse, x forward, y inverse and y forward

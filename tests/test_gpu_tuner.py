@@ -55,3 +55,21 @@ def test_tuned_schedule_is_the_fastest_timed(dns_lib, tmp_path):
         cands = part.split("{")[1].rstrip("}").split(", ")
         times = {int(c.split(":")[0]): float(c.split(": ")[1].split(" ")[0]) for c in cands}
         assert times[chosen] == min(times.values()), part
+
+
+def test_batch_is_tuned_on_its_run_count(dns_lib):
+    """An ensemble group is tuned on its own batch (up to the volume of two
+    256^3 runs): the schedule names the run count, and each pick is the
+    fastest candidate timed on it."""
+    import dns_b200
+
+    with dns_b200.Ensemble([64] * 4 + [128] * 2, dns_b200.DNS_PREC_MIXED) as ens:
+        s = ens.schedule()
+    for n, runs in ((64, 4), (128, 2)):
+        part = s.split(f"; n={n}: ")[1].split("; n=")[0]
+        assert part.startswith(f"timed on {runs} runs: "), s
+        for p in part[len(f"timed on {runs} runs: "):].split("; "):
+            chosen = int(p.split("min blocks/SM ")[1].split(" ")[0])
+            cands = p.split("{")[1].rstrip("}").split(", ")
+            times = {int(c.split(":")[0]): float(c.split(": ")[1].split(" ")[0]) for c in cands}
+            assert times[chosen] == min(times.values()), p
