@@ -1044,9 +1044,41 @@ double binom(int n, int k) {
   return r;
 }
 
+// binomial split of steps [a, b) with `free` spare snapshots (b - a >= 2,
+// free >= 1): smallest repetition number rr with C(free + rr, free) >= l;
+// the right part [m, b) gets what free - 1 snapshots reverse in rr
+long adj_split(long a, long b, int free) {
+  const long l = b - a;
+  int rr = 0;
+  while (binom(free + rr, free) < (double)l) rr++;
+  const double right_cap = binom(free - 1 + rr, free - 1);
+  long lr = right_cap < (double)(l - 1) ? (long)right_cap : l - 1;
+  if (lr < 1) lr = 1;
+  return b - lr;
+}
+
+// forward sweep over steps [0, b) from the state in snapshot 0, storing
+// the snapshots of the reverse sweep's rightmost path (the split points
+// adj_reverse takes first, each with one snapshot fewer) on the way, so
+// the reverse sweep need not recompute them
+int adj_sweep(Adj &A, long b, int free) {
+  long a = 0;
+  int ka = 0, r;
+  while (b - a >= 2 && free >= 1) {
+    const long m = adj_split(a, b, free);
+    if ((r = adj_advance(A, m - a))) return r;
+    if ((r = adj_snap_store(A, ka + 1))) return r;
+    a = m;
+    ka++;
+    free--;
+  }
+  return adj_advance(A, b - a);
+}
+
 // reverse steps [a, b): the state at step a is in snapshot ka; snapshots
-// ka+1 .. ka+free are unused
-int adj_reverse(Adj &A, long a, long b, int ka, int free) {
+// ka+1 .. ka+free are unused, unless `stored`: then those of the rightmost
+// path of the split tree are already in place (adj_sweep)
+int adj_reverse(Adj &A, long a, long b, int ka, int free, bool stored) {
   int r;
   if (b - a == 1) {
     if ((r = adj_snap_restore(A, ka))) return r;
@@ -1060,20 +1092,14 @@ int adj_reverse(Adj &A, long a, long b, int ka, int free) {
     }
     return DNS_OK;
   }
-  // binomial split: smallest repetition number rr with C(free + rr, free)
-  // >= l; the right part gets what free - 1 snapshots reverse in rr
-  const long l = b - a;
-  int rr = 0;
-  while (binom(free + rr, free) < (double)l) rr++;
-  const double right_cap = binom(free - 1 + rr, free - 1);
-  long lr = right_cap < (double)(l - 1) ? (long)right_cap : l - 1;
-  if (lr < 1) lr = 1;
-  const long m = b - lr;
-  if ((r = adj_snap_restore(A, ka))) return r;
-  if ((r = adj_advance(A, m - a))) return r;
-  if ((r = adj_snap_store(A, ka + 1))) return r;
-  if ((r = adj_reverse(A, m, b, ka + 1, free - 1))) return r;
-  return adj_reverse(A, a, m, ka, free);
+  const long m = adj_split(a, b, free);
+  if (!stored) {
+    if ((r = adj_snap_restore(A, ka))) return r;
+    if ((r = adj_advance(A, m - a))) return r;
+    if ((r = adj_snap_store(A, ka + 1))) return r;
+  }
+  if ((r = adj_reverse(A, m, b, ka + 1, free - 1, stored))) return r;
+  return adj_reverse(A, a, m, ka, free, false);
 }
 
 int ctx_build_graph(dns_ctx *c) {
@@ -1771,9 +1797,13 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     }
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
+  // J alone: the forward sweep is all it takes (no snapshots are needed
+  // beyond the first, and no reverse sweep runs)
+  const bool want_grad = gU || gV || gW || gnu;
   if (r == DNS_OK) r = set_velocity_view(A.G, A.st, U, V, W);
   if (r == DNS_OK) r = adj_snap_store(A, 0);
-  if (r == DNS_OK) r = adj_advance(A, nsteps);  // forward sweep to T
+  if (r == DNS_OK)  // forward sweep to T
+    r = want_grad ? adj_sweep(A, nsteps, snapshots - 1) : adj_advance(A, nsteps);
   double4 d = make_double4(0, 0, 0, 0);
   const double invn3 = 1.0 / (double)g.nreal;
   if (r == DNS_OK) {
@@ -1782,9 +1812,6 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     if (e == cudaSuccess) e = cudaStreamSynchronize(A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
-  // J alone: the forward sweep is all it takes (no snapshots are needed
-  // beyond the first, and no reverse sweep runs)
-  const bool want_grad = gU || gV || gW || gnu;
   if (r == DNS_OK && !want_grad) {
     if (J) *J = (d.x + d.y) * (invn3 * invn3);
     cleanup();
@@ -1801,7 +1828,7 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3d(), A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
-  if (r == DNS_OK) r = adj_reverse(A, 0, nsteps, 0, snapshots - 1);
+  if (r == DNS_OK) r = adj_reverse(A, 0, nsteps, 0, snapshots - 1, true);
   if (r == DNS_OK) {
     // dE/du0 = r2c^T(lambda_U(0)) + lambda_stale(0) = c2r(lambda / w_z) + lambda_stale
     const int t3[3] = {0, 1, 2};
