@@ -119,31 +119,38 @@ __global__ void k_adj_cross(const RU *__restrict__ u, const double *__restrict__
   }
 }
 
-// lUs = a w_z (curl(Rw) + Ru) - nu dt kk ldU       (Ru may be null: stage 0)
-// and the nu-gradient terms <ldU, -dt kk Us>, double-double block partials
+// lUs = a w_z (curl(Rw) + Ru) - nu dt kk ldU       (Ru may be null: stage 0),
+// the adjoint of the stage input U_s = U0 + b dU_{s-1}, consumed at once:
+//   lhat_out = lhat_in + lUs                (lambda of U0, accumulated)
+//   ldU      = bn lUs + an lacc             (lambda of dU_{s-1}; not at stage 0)
+// with ldU overwritten in place; and the nu-gradient terms <ldU, -dt kk Us>,
+// double-double block partials
 template <int BS, class C>
 __global__ void __launch_bounds__(BS)
-    k_adj_collect(const C *__restrict__ Rw, const C *__restrict__ Ru, const C *__restrict__ ldU,
-                  const C *__restrict__ Us, C *__restrict__ out, Geo g, double a, double nu,
-                  double dt, double4 *__restrict__ partial) {
+    k_adj_collect(const C *__restrict__ Rw, const C *__restrict__ Ru, C *ldU,
+                  const C *__restrict__ Us, const C *lhat_in, C *lhat_out,
+                  const C *__restrict__ lacc, Geo g, double a, double nu, double dt, double bn,
+                  double an, bool next, double4 *__restrict__ partial) {
   DD gn{0.0, 0.0}, unused{0.0, 0.0};
   DNSB_FOR_POINTS(g) {
     const PointK p = point_k(g, q);
-    cd cx, cy, cz;
-    curl_at(p, to_d(Rw[p.o]), to_d(Rw[g.slot + p.o]), to_d(Rw[2 * g.slot + p.o]), cx, cy, cz);
-    if (Ru) {
-      cx = cadd(cx, to_d(Ru[p.o]));
-      cy = cadd(cy, to_d(Ru[g.slot + p.o]));
-      cz = cadd(cz, to_d(Ru[2 * g.slot + p.o]));
-    }
+    cd cxyz[3];
+    curl_at(p, to_d(Rw[p.o]), to_d(Rw[g.slot + p.o]), to_d(Rw[2 * g.slot + p.o]), cxyz[0],
+            cxyz[1], cxyz[2]);
     const double s = a * p.wz, c = nu * dt * p.kk;
-    const cd lx = to_d(ldU[p.o]), ly = to_d(ldU[g.slot + p.o]), lz = to_d(ldU[2 * g.slot + p.o]);
-    out[p.o] = from_d<C>(make_double2(s * cx.x - c * lx.x, s * cx.y - c * lx.y));
-    out[g.slot + p.o] = from_d<C>(make_double2(s * cy.x - c * ly.x, s * cy.y - c * ly.y));
-    out[2 * g.slot + p.o] = from_d<C>(make_double2(s * cz.x - c * lz.x, s * cz.y - c * lz.y));
-    const cd ux = to_d(Us[p.o]), uy = to_d(Us[g.slot + p.o]), uz = to_d(Us[2 * g.slot + p.o]);
-    const double dotp = lx.x * ux.x + lx.y * ux.y + ly.x * uy.x + ly.y * uy.y + lz.x * uz.x +
-                        lz.y * uz.y;
+    double dotp = 0.0;
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      const long long o = f * g.slot + p.o;
+      cd cf = cxyz[f];
+      if (Ru) cf = cadd(cf, to_d(Ru[o]));
+      const cd l = to_d(ldU[o]), u = to_d(Us[o]);
+      dotp += l.x * u.x;
+      dotp += l.y * u.y;
+      const cd lus = make_double2(s * cf.x - c * l.x, s * cf.y - c * l.y);
+      lhat_out[o] = from_d<C>(cadd(to_d(lhat_in[o]), lus));
+      if (next) ldU[o] = from_d<C>(cadd(cscale(lus, bn), cscale(to_d(lacc[o]), an)));
+    }
     gn = dd_add_d(gn, -dt * p.kk * dotp);
   }
   dd_block_reduce<BS>(gn, unused, partial + blockIdx.x);

@@ -904,11 +904,12 @@ int set_coef(const Group &G, cudaStream_t st, const double *nu, const double *dt
 // (U_hat, stale velocity) follow a binomial split of the step range.
 // ---------------------------------------------------------------------------
 // spectral work triples (in units of slots)
-enum { X_US0 = 0, X_LHAT = 12, X_LACC = 15, X_LDU = 18, X_LHAT0 = 21, X_LUS = 24, X_T1 = 27,
-       X_T2 = 30, NX = 33 };
+// (the stage inputs U_1..U_3; two buffers for lambda of the step state, one
+// holding the step output's, the other accumulating the step input's, which
+// swap roles after every reversed step; lambda of dU_s; two transform triples)
+enum { X_US1 = 0, X_LA = 9, X_LB = 12, X_LDU = 15, X_T1 = 18, X_T2 = 21, NX = 24 };
 // real work triples (in units of n^3 fields)
-enum { RE_U = 0, RE_OM = 3, RE_LN = 6, RE_LU = 9, RE_LOM = 12, RE_LSTALE = 15, RE_STALEIN = 18,
-       NRE = 21 };
+enum { RE_U = 0, RE_OM = 3, RE_LN = 6, RE_LU = 9, RE_LOM = 12, RE_LSTALE = 15, NRE = 18 };
 
 struct Adj {
   Group G;
@@ -916,12 +917,13 @@ struct Adj {
   cudaGraphExec_t graph = nullptr;
   char *arena = nullptr;
   void *sp = nullptr;        // [NX][slot], storage complex type
-  double *re = nullptr;      // [NRE][n^3] float64; LU, LOM, STALEIN hold the storage real type
+  double *re = nullptr;      // [NRE][n^3] float64; LU, LOM hold the storage real type
   char *snap_sp = nullptr;   // [S][3][slot]
   char *snap_re = nullptr;   // [S][3][n^3], storage real type
   double4 *part = nullptr, *acc_nu = nullptr;
   int nblocks = 0;
   double nu = 0, dt = 0;
+  int lhat = X_LA;  // the buffer holding lambda of the current step state
   template <class C>
   C *X(int i) const { return (C *)sp + (size_t)i * G.g.slot; }
   double *Rf(int i) const { return re + (size_t)i * G.g.nreal; }
@@ -943,14 +945,21 @@ struct AdjOps {
   }
   static unsigned pblocks(const Adj &A) { return (unsigned)A.nblocks; }
 
-  // adjoint of RK stage s: from lambda_dU (X_LDU) and U_s (X_US0 + 3 s)
-  // produce lambda_{U_s} (X_LUS); stage 0 also produces lambda_stale
-  static int stage(Adj &A, int s) {
+  // U_s: the step input (slot SA, untouched by the forward stages 0-2) or a
+  // kept stage input
+  static const C *stage_input(const Adj &A, int s) {
+    return s == 0 ? (const C *)A.G.slot_ptr(0, SLOT_SA) : A.X<C>(X_US1 + 3 * (s - 1));
+  }
+
+  // adjoint of RK stage s: from lambda_dU (X_LDU) and U_s, add lambda_{U_s}
+  // to lambda of U0 (lin into lout) and, for s > 0, form lambda_dU of stage
+  // s - 1 in X_LDU; stage 0 also produces lambda_stale
+  static int stage(Adj &A, int s, const C *lin, C *lout, const C *lacc) {
     const Group &G = A.G;
     const Geo &g = G.g;
     const double a = 1.0 / (double)g.nreal;
     const int t3[3] = {0, 1, 2};
-    const C *Us = A.X<C>(X_US0 + 3 * s);
+    const C *Us = stage_input(A, s);
     if (s > 0) O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
     const unsigned pb = pblocks(A);
     k_curl<C><<<pb, 256, 0, A.st>>>(Us, A.X<C>(X_T1), g);
@@ -961,15 +970,15 @@ struct AdjOps {
       k_adj_cross<double, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
           A.Rf(RE_U), A.Rf(RE_OM), A.Rf(RE_LN), s == 3 ? A.Rf(RE_LSTALE) : nullptr,
           A.Rr<R>(RE_LU), A.Rr<R>(RE_LOM), g.nreal);
-    else  // stage 0 reads the stale velocity (main.c:344)
+    else  // stage 0 reads the stale velocity (main.c:344), the step's input one
       k_adj_cross<R, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
-          A.Rr<R>(RE_STALEIN), A.Rf(RE_OM), A.Rf(RE_LN), nullptr, A.Rr<R>(RE_LU),
+          (const R *)G.stale, A.Rf(RE_OM), A.Rf(RE_LN), nullptr, A.Rr<R>(RE_LU),
           A.Rr<R>(RE_LOM), g.nreal);
     O::r2c_fields(G, A.st, A.Rr<R>(RE_LOM), 3, A.X<C>(X_T1), t3);
     if (s > 0) O::r2c_fields(G, A.st, A.Rr<R>(RE_LU), 3, A.X<C>(X_T2), t3);
-    k_adj_collect<256, C><<<pb, 256, 0, A.st>>>(A.X<C>(X_T1), s > 0 ? A.X<C>(X_T2) : nullptr,
-                                                A.X<C>(X_LDU), Us, A.X<C>(X_LUS), g, a, A.nu, A.dt,
-                                                A.part);
+    k_adj_collect<256, C><<<pb, 256, 0, A.st>>>(
+        A.X<C>(X_T1), s > 0 ? A.X<C>(X_T2) : nullptr, A.X<C>(X_LDU), Us, lin, lout, lacc, g, a,
+        A.nu, A.dt, s > 0 ? RK_B[s - 1] : 0.0, s > 0 ? RK_A[s - 1] : 0.0, s > 0, A.part);
     k_dd_accumulate<256><<<1, 256, 0, A.st>>>(A.part, A.nblocks, A.acc_nu);
     if (s == 0)  // lambda of the step's input stale velocity, kept in float64
       k_real_convert<R, double><<<conv_blocks(3 * g.nreal), 256, 0, A.st>>>(
@@ -979,33 +988,27 @@ struct AdjOps {
   }
 
   // adjoint of one step whose input state is in (SA, stale); lambda of the
-  // step output in (X_LHAT, RE_LSTALE) becomes lambda of its input
+  // step output in (A.lhat, RE_LSTALE) becomes lambda of its input (in the
+  // other buffer, which becomes A.lhat).  The forward stages 0-2 run again
+  // to recover the stage inputs U_1..U_3 (stage 3's output is not needed);
+  // the step's state (SA, stale) is left in place for stage 0's adjoint.
   static int step(Adj &A) {
     const Group &G = A.G;
     const Geo &g = G.g;
-    const unsigned pb = pblocks(A);
     int r;
-    if ((r = copy3(A, A.X<C>(X_US0), G.slot_ptr(0, SLOT_SA), A.slot3()))) return r;
-    if ((r = copy3(A, A.Rr<R>(RE_STALEIN), G.stale, A.real3()))) return r;
-    for (int s = 0; s < 4; s++) {  // forward again, keeping the stage inputs
+    for (int s = 0; s < 3; s++) {
       for (int k = 0; k < KERNELS_PER_STAGE; k++) O::stage_kernel(G, A.st, s, k);
-      if (s < 3 && (r = copy3(A, A.X<C>(X_US0 + 3 * (s + 1)), G.slot_ptr(0, SLOT_SB), A.slot3())))
-        return r;
+      if ((r = copy3(A, A.X<C>(X_US1 + 3 * s), G.slot_ptr(0, SLOT_SB), A.slot3()))) return r;
     }
-    if ((r = copy3(A, A.X<C>(X_LACC), A.X<C>(X_LHAT), A.slot3()))) return r;
-    if ((r = copy3(A, A.X<C>(X_LHAT0), A.X<C>(X_LHAT), A.slot3()))) return r;  // acc_0 = U0
-    for (int s = 3; s >= 0; s--) {
-      if (s == 3)
-        k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LACC), nullptr, A.X<C>(X_LDU), g, RK_A[3], 0.0);
-      else  // U_{s+1} = U0 + b_s dU_s, acc += a_s dU_s
-        k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LUS), A.X<C>(X_LACC), A.X<C>(X_LDU), g,
-                                            RK_B[s], RK_A[s]);
-      if ((r = stage(A, s))) return r;
-      // every stage input U_s is U0 plus a multiple of dU_{s-1}
-      k_lincomb3<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LHAT0), A.X<C>(X_LUS), A.X<C>(X_LHAT0), g, 1.0,
-                                          1.0);
-    }
-    if ((r = copy3(A, A.X<C>(X_LHAT), A.X<C>(X_LHAT0), A.slot3()))) return r;
+    const int lo = A.lhat, li = A.lhat == X_LA ? X_LB : X_LA;
+    const C *lacc = A.X<C>(lo);  // lambda of the accumulator: that of the step output
+    // lambda_dU of stage 3 = a_3 lambda_acc
+    k_lincomb3<C><<<pblocks(A), 256, 0, A.st>>>(lacc, nullptr, A.X<C>(X_LDU), g, RK_A[3], 0.0);
+    // lambda of U0 = lambda of the output (through the accumulator's U0 term)
+    // plus the lambda of every stage input (each U0 plus a multiple of dU)
+    for (int s = 3; s >= 0; s--)
+      if ((r = stage(A, s, s == 3 ? lacc : A.X<C>(li), A.X<C>(li), lacc))) return r;
+    A.lhat = li;
     CKL();
     return DNS_OK;
   }
@@ -1823,7 +1826,7 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     dispatch(A.G, [&](auto ops) {
       using C = typename decltype(ops)::C;
       k_lincomb3<C><<<A.nblocks, 256, 0, A.st>>>((const C *)A.G.slot_ptr(0, SLOT_SA), nullptr,
-                                                 A.X<C>(X_LHAT), g, 2.0 * invn3 * invn3, 0.0);
+                                                 A.X<C>(A.lhat), g, 2.0 * invn3 * invn3, 0.0);
     });
     cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3d(), A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
@@ -1835,7 +1838,7 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     dispatch(A.G, [&](auto ops) {
       using O = decltype(ops);
       using C = typename O::C;
-      k_div_wz3<C><<<A.nblocks, 256, 0, A.st>>>(A.X<C>(X_LHAT), A.X<C>(X_T1), g);
+      k_div_wz3<C><<<A.nblocks, 256, 0, A.st>>>(A.X<C>(A.lhat), A.X<C>(X_T1), g);
       O::c2r_fields(A.G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
     });
     k_add_real<<<conv_blocks(3 * g.nreal), 256, 0, A.st>>>(A.Rf(RE_LSTALE), A.Rf(RE_LN), 3 * g.nreal);
