@@ -93,10 +93,10 @@ __global__ void k_adj_lamN(const C *__restrict__ ldU, C *__restrict__ out, Geo g
   }
 }
 
-// lu = om x lN (+ lstale_out), lom = lN x u   on [3][n^3] real arrays (u
-// and the outputs in the storage precision, the rest float64)
-template <class RU, class RO>
-__global__ void k_adj_cross(const RU *__restrict__ u, const double *__restrict__ om,
+// lu = om x lN (+ lstale_out), lom = lN x u   on [3][n^3] real arrays (u,
+// om and the outputs in the precision they are kept in, the rest float64)
+template <class RU, class RW, class RO>
+__global__ void k_adj_cross(const RU *__restrict__ u, const RW *__restrict__ om,
                             const double *__restrict__ lN, const double *__restrict__ lstale_out,
                             RO *__restrict__ lu, RO *__restrict__ lom, long long nr) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nr;

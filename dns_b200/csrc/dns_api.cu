@@ -224,6 +224,8 @@ struct Ops {
   static constexpr size_t Z_SMEM = (size_t)(2 * N + ZCfg<N>::LINES * ZCfg<N>::XB) * sizeof(C);
   template <int KIND>
   static constexpr size_t ZS_SMEM = ZC<R, N, KIND>::SMEM;
+  // the z pass can keep its real velocity and vorticity (k_zstage_keep)
+  static constexpr bool ZKEEP = ZC<R, N, 1>::S2 || ZC<R, N, 1>::F32;
 
   // Column-pass register schedules.  Candidate I of a pass is the same
   // kernel compiled with a minimum of ColCands::m[I] resident blocks per SM
@@ -289,6 +291,10 @@ struct Ops {
     if ((e = allow(k_zstage<R, N, 0>, ZS_SMEM<0>))) return e;
     if ((e = allow(k_zstage<R, N, 1>, ZS_SMEM<1>))) return e;
     if ((e = allow(k_zstage<R, N, 2>, ZS_SMEM<2>))) return e;
+    if constexpr (ZKEEP) {
+      if ((e = allow(k_zstage_keep<R, N, 0>, ZS_SMEM<0>))) return e;
+      if ((e = allow(k_zstage_keep<R, N, 1>, ZS_SMEM<1>))) return e;
+    }
     if ((e = allow(k_zr2c<R, N>, Z_SMEM))) return e;
     if ((e = allow(k_zc2r<R, N>, Z_SMEM))) return e;
     return cudaSuccess;
@@ -419,6 +425,20 @@ struct Ops {
   static void zpass(const Group &G, cudaStream_t st, C *work, R *stale, R invn3) {
     k_zstage<R, N, KIND><<<zsgrid<KIND>(G.nruns), ZC<R, N, KIND>::THREADS, ZS_SMEM<KIND>, st>>>(
         work, stale, tw(G), G.g, invn3);
+  }
+  // the z pass of RK stage s of one run (the first stage's or the middle
+  // stages' form), keeping the real velocity and vorticity in keep[6][n^3]
+  static void zpass_keep(const Group &G, cudaStream_t st, int s, R *keep) {
+    if constexpr (ZKEEP) {
+      C *work = slot(G, SLOT_WORK);
+      const R invn3 = (R)(1.0 / (double)G.g.nreal);
+      if (s == 0)
+        k_zstage_keep<R, N, 0><<<zsgrid<0>(1), ZC<R, N, 0>::THREADS, ZS_SMEM<0>, st>>>(
+            work, (R *)G.stale, tw(G), G.g, invn3, keep);
+      else
+        k_zstage_keep<R, N, 1><<<zsgrid<1>(1), ZC<R, N, 1>::THREADS, ZS_SMEM<1>, st>>>(
+            work, (R *)G.stale, tw(G), G.g, invn3, keep);
+    }
   }
 
   static C *slot(const Group &G, int s) { return (C *)G.S + (long long)s * G.g.slot; }
@@ -920,6 +940,8 @@ struct Adj {
   double *re = nullptr;      // [NRE][n^3] float64; LU, LOM hold the storage real type
   char *snap_sp = nullptr;   // [S][3][slot]
   char *snap_re = nullptr;   // [S][3][n^3], storage real type
+  char *keep = nullptr;      // [4][6][n^3], storage real type: the real velocity and
+                             // vorticity of each RK stage, where the z pass keeps them
   double4 *part = nullptr, *acc_nu = nullptr;
   int nblocks = 0;
   double nu = 0, dt = 0;
@@ -933,6 +955,8 @@ struct Adj {
   size_t slot3() const { return (size_t)3 * G.g.slot * G.csize; }
   size_t real3() const { return (size_t)3 * G.g.nreal * G.rsize; }
   size_t real3d() const { return (size_t)3 * G.g.nreal * sizeof(double); }
+  template <class R>
+  R *K(int s, int f) const { return (R *)keep + ((size_t)6 * s + f) * G.g.nreal; }
 };
 
 template <class R, int N>
@@ -960,20 +984,29 @@ struct AdjOps {
     const double a = 1.0 / (double)g.nreal;
     const int t3[3] = {0, 1, 2};
     const C *Us = stage_input(A, s);
-    if (s > 0) O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
     const unsigned pb = pblocks(A);
-    k_curl<C><<<pb, 256, 0, A.st>>>(Us, A.X<C>(X_T1), g);
-    O::c2r_fields(G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_OM), a);
+    if constexpr (!O::ZKEEP) {  // the velocity and vorticity of the stage, again
+      if (s > 0) O::c2r_fields(G, A.st, Us, t3, 3, A.Rf(RE_U), a);
+      k_curl<C><<<pb, 256, 0, A.st>>>(Us, A.X<C>(X_T1), g);
+      O::c2r_fields(G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_OM), a);
+    }
     k_adj_lamN<C><<<pb, 256, 0, A.st>>>(A.X<C>(X_LDU), A.X<C>(X_T1), g, A.dt);
     O::c2r_fields(G, A.st, A.X<C>(X_T1), t3, 3, A.Rf(RE_LN), 1.0);
-    if (s > 0)
-      k_adj_cross<double, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
-          A.Rf(RE_U), A.Rf(RE_OM), A.Rf(RE_LN), s == 3 ? A.Rf(RE_LSTALE) : nullptr,
-          A.Rr<R>(RE_LU), A.Rr<R>(RE_LOM), g.nreal);
-    else  // stage 0 reads the stale velocity (main.c:344), the step's input one
-      k_adj_cross<R, R><<<conv_blocks(g.nreal), 256, 0, A.st>>>(
-          (const R *)G.stale, A.Rf(RE_OM), A.Rf(RE_LN), nullptr, A.Rr<R>(RE_LU),
-          A.Rr<R>(RE_LOM), g.nreal);
+    const double *lso = s == 3 ? A.Rf(RE_LSTALE) : nullptr;
+    const unsigned cb = conv_blocks(g.nreal);
+    // stage 0 reads the stale velocity (main.c:344), the step's input one
+    if constexpr (O::ZKEEP) {  // kept by the z pass of the forward stage
+      const R *u = s > 0 ? A.K<R>(s, 0) : (const R *)G.stale;
+      k_adj_cross<R, R, R><<<cb, 256, 0, A.st>>>(u, A.K<R>(s, 3), A.Rf(RE_LN), lso,
+                                                 A.Rr<R>(RE_LU), A.Rr<R>(RE_LOM), g.nreal);
+    } else if (s > 0) {
+      k_adj_cross<double, double, R><<<cb, 256, 0, A.st>>>(
+          A.Rf(RE_U), A.Rf(RE_OM), A.Rf(RE_LN), lso, A.Rr<R>(RE_LU), A.Rr<R>(RE_LOM), g.nreal);
+    } else {
+      k_adj_cross<R, double, R><<<cb, 256, 0, A.st>>>((const R *)G.stale, A.Rf(RE_OM),
+                                                      A.Rf(RE_LN), lso, A.Rr<R>(RE_LU),
+                                                      A.Rr<R>(RE_LOM), g.nreal);
+    }
     O::r2c_fields(G, A.st, A.Rr<R>(RE_LOM), 3, A.X<C>(X_T1), t3);
     if (s > 0) O::r2c_fields(G, A.st, A.Rr<R>(RE_LU), 3, A.X<C>(X_T2), t3);
     k_adj_collect<256, C><<<pb, 256, 0, A.st>>>(
@@ -992,13 +1025,24 @@ struct AdjOps {
   // other buffer, which becomes A.lhat).  The forward stages 0-2 run again
   // to recover the stage inputs U_1..U_3 (stage 3's output is not needed);
   // the step's state (SA, stale) is left in place for stage 0's adjoint.
+  // Where the z pass can keep its real velocity and vorticity, every stage's
+  // z pass (stage 3's too, after its A and B passes; without its stale
+  // store) keeps them for the transposed stage.
   static int step(Adj &A) {
     const Group &G = A.G;
     const Geo &g = G.g;
     int r;
-    for (int s = 0; s < 3; s++) {
-      for (int k = 0; k < KERNELS_PER_STAGE; k++) O::stage_kernel(G, A.st, s, k);
-      if ((r = copy3(A, A.X<C>(X_US1 + 3 * s), G.slot_ptr(0, SLOT_SB), A.slot3()))) return r;
+    for (int s = 0; s < 4; s++) {
+      if (!O::ZKEEP && s == 3) break;
+      for (int k = 0; k < KERNELS_PER_STAGE; k++) {
+        if (s == 3 && k > 2) break;
+        if (O::ZKEEP && k == 2)
+          O::zpass_keep(G, A.st, s, A.K<R>(s, 0));
+        else
+          O::stage_kernel(G, A.st, s, k);
+      }
+      if (s < 3 && (r = copy3(A, A.X<C>(X_US1 + 3 * s), G.slot_ptr(0, SLOT_SB), A.slot3())))
+        return r;
     }
     const int lo = A.lhat, li = A.lhat == X_LA ? X_LB : X_LA;
     const C *lacc = A.X<C>(lo);  // lambda of the accumulator: that of the step output
@@ -1768,9 +1812,14 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     const size_t re_b = (size_t)NRE * g.nreal * sizeof(double);
     const size_t ssp_b = (size_t)snapshots * A.slot3();
     const size_t sre_b = (size_t)snapshots * A.real3();
+    const size_t keep_b = (size_t)24 * g.nreal * A.G.rsize;
     const size_t part_b = (size_t)(A.nblocks + 1) * sizeof(double4);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    cudaError_t e = cudaMalloc((void **)&A.arena, al(sp_b) + al(re_b) + al(ssp_b) + al(sre_b) + al(part_b));
+    bool zkeep = false;
+    dispatch(A.G, [&](auto ops) { zkeep = decltype(ops)::ZKEEP; });
+    const size_t keep_a = zkeep ? al(keep_b) : 0;
+    cudaError_t e = cudaMalloc((void **)&A.arena,
+                               al(sp_b) + al(re_b) + al(ssp_b) + al(sre_b) + keep_a + al(part_b));
     if (e != cudaSuccess) {
       A.arena = nullptr;
       r = fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
@@ -1780,6 +1829,10 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
       A.re = (double *)p; p += al(re_b);
       A.snap_sp = p; p += al(ssp_b);
       A.snap_re = p; p += al(sre_b);
+      if (zkeep) {
+        A.keep = p;
+        p += keep_a;
+      }
       A.part = (double4 *)p;
       A.acc_nu = A.part + A.nblocks;
       e = cudaMemsetAsync(A.arena, 0, al(sp_b) + al(re_b), A.st);

@@ -598,11 +598,15 @@ __device__ __forceinline__ void zstage_forward(cx<R> (&y)[ZC<R, N, KIND>::E],
 
 // One block of the z pass: Z::LINES lines starting at line b.x * LINES of
 // run b.y (block-wide barriers through `bsync`, which lines of more than 32
-// threads also use between FFT stages).
-template <class R, int N, int KIND, class BSync>
+// threads also use between FFT stages).  KEEP (the pair orders of S2 and
+// FP32 only): also store the real velocity and vorticity the pass forms in
+// keep[f][n^3], f = u, v, w, omega_x, omega_y, omega_z of the run (the
+// first stage: the vorticity only), for the discrete adjoint.
+template <class R, int N, int KIND, bool KEEP = false, class BSync>
 __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restrict__ stale,
                                             const cx<R> *__restrict__ twg, const Geo &g, R invn3,
-                                            const Blk b, BSync bsync, unsigned char *smem) {
+                                            const Blk b, BSync bsync, unsigned char *smem,
+                                            R *__restrict__ keep = nullptr) {
   using C = cx<R>;
   using Z = ZC<R, N, KIND>;
   constexpr int E = Z::E, T = Z::T;
@@ -618,6 +622,7 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
   const bool ok = line < (long long)N * N;
   work += (long long)b.y * g.run_spec;  // run of the batch
   stale += (long long)b.y * g.run_real;
+  if constexpr (KEEP) keep += (long long)b.y * 6 * g.nreal;
   const long long off = line * g.nfp;
   const C *pU = work + SU * g.slot + off, *pV = work + SV * g.slot + off;
   const C *pW = work + SW * g.slot + off, *pOMZ = work + SOMZ * g.slot + off;
@@ -648,6 +653,11 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
   const LineSync<(T > 32), BSync> sync{bsync};
   const PadShift<Z::PADSH> idx{};
   const long long roff = line * N;
+  auto kp = [&](int f, int e, R v) {
+    if constexpr (KEEP) {
+      if (ok) keep[f * g.nreal + roff + t + T * e] = v;
+    }
+  };
 
   C y[E];
   if constexpr (Z::S2 || Z::F32) {
@@ -670,6 +680,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
         nx[e] = -w * oy;
         ny[e] = w * ox;
         y[e] = cmk<C>(u * oy - v * ox, R(0));  // N_z
+        kp(3, e, ox);
+        kp(4, e, oy);
       }
       zfwd_z<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
       ext_pair<R, N, KIND>(y, t, f_oz, f_zero);
@@ -678,6 +690,7 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
       for (int e = 0; e < E; e++) {
         const R oz = y[e].x * invn3;
         y[e] = cmk<C>(nx[e] + sv(1, e) * oz, ny[e] - sv(0, e) * oz);  // (N_x, N_y)
+        kp(5, e, oz);
       }
       zfwd_xy<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
     } else {
@@ -705,6 +718,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
           soy[e] = oy;
         }
         if (KIND == 2 && ok) stale[roff + t + T * e] = u;
+        kp(0, e, u);
+        kp(4, e, oy);
       }
       auto U_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(0, e); else return su[e]; };
       auto OY_ = [&](int e) -> R { if constexpr (Z::S2) return SU_(1, e); else return soy[e]; };
@@ -725,6 +740,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
         const R nz = U_(e) * OY_(e);
         y[e] = cmk<C>(nz - v * ox, R(0));  // N_z
         if (KIND == 2 && ok) stale[g.nreal + roff + t + T * e] = v;
+        kp(1, e, v);
+        kp(3, e, ox);
       }
       zfwd_z<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
       ext_gen<R, N, KIND>(y, t, [&](int s, C &a, C &b) {
@@ -738,6 +755,8 @@ __device__ __forceinline__ void zstage_body(cx<R> *__restrict__ work, R *__restr
         const R nx = -w * OY_(e), ny = -U_(e) * oz;
         y[e] = cmk<C>(nx + sv_[e] * oz, ny + w * sox[e]);  // (N_x, N_y)
         if (KIND == 2 && ok) stale[2 * g.nreal + roff + t + T * e] = w;
+        kp(2, e, w);
+        kp(5, e, oz);
       }
       zfwd_xy<R, N, KIND>(y, t, tw, xb, idx, sync, work + off, g, ok);
     }
@@ -876,6 +895,19 @@ __global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
              R invn3) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   zstage_body<R, N, KIND>(work, stale, twg, g, invn3, launch_blk(), BlockSync{}, smem_raw);
+}
+
+// The z pass that also keeps the real velocity and vorticity (KEEP above),
+// for the forward recomputation of the discrete adjoint; the pair orders of
+// S2 and FP32 only.
+template <class R, int N, int KIND>
+__global__ void __launch_bounds__(ZC<R, N, KIND>::THREADS, ZC<R, N, KIND>::MINB)
+    k_zstage_keep(cx<R> *__restrict__ work, R *__restrict__ stale, const cx<R> *__restrict__ twg,
+                  Geo g, R invn3, R *__restrict__ keep) {
+  static_assert(ZC<R, N, KIND>::S2 || ZC<R, N, KIND>::F32, "KEEP needs the S2 or FP32 pair order");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  zstage_body<R, N, KIND, true>(work, stale, twg, g, invn3, launch_blk(), BlockSync{}, smem_raw,
+                                keep);
 }
 
 // ---------------------------------------------------------------------------
