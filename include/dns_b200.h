@@ -226,8 +226,11 @@ int dns_ens_synchronize(dns_ens *e);
  * nu (gnu).  FP64.  The transposed step is hand-written; forward states are
  * recomputed from `snapshots` stored step states (>= 1, the initial state
  * included) placed by a binomial split of the step range, so memory is
- * independent of nsteps.  Any output pointer may be NULL; with all four
- * gradient pointers NULL only the forward sweep runs (J alone). */
+ * independent of nsteps: the snapshots (3 spectral and 3 real fields each)
+ * plus a fixed work set (41 spectral and 45 real fields, the step's own
+ * state included; 256^3 FP64 with 20 snapshots: about 28 GB).  Any output pointer may be NULL;
+ * with all four gradient pointers NULL only the forward sweep runs (J
+ * alone). */
 int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,
                        double dt, long nsteps, int snapshots, double *J, double *gU, double *gV,
                        double *gW, double *gnu);
