@@ -259,6 +259,7 @@ struct Ops {
     float ms[2][2][16];
   };
   static inline std::map<int, TuneRec> tune_cache;
+  static inline std::mutex tune_mu;  // guards tune_cache
   template <int AXIS, bool FWD>
   static ColFn colkern(const Group &G) {
     return col_cand_at<AXIS, FWD>(G.pick[AXIS][FWD]);
@@ -345,8 +346,7 @@ struct Ops {
   // dns_get_schedule reports them; a value that is not a candidate means
   // the compiler's).
   static cudaError_t tune(Group &G, cudaStream_t st, bool *ran) {
-    static std::mutex mu;
-    std::lock_guard<std::mutex> lock(mu);
+    std::lock_guard<std::mutex> lock(tune_mu);
     *ran = false;
     G.tune_runs = tune_runs(G.nruns);
     auto it = tune_cache.find(G.tune_runs);
@@ -398,6 +398,7 @@ struct Ops {
     TuneRec rec{};
     memcpy(rec.pick, G.pick, sizeof rec.pick);
     {
+      std::lock_guard<std::mutex> lock(tune_mu);
       auto it = tune_cache.find(G.tune_runs);
       if (it != tune_cache.end()) rec = it->second;
     }
