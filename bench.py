@@ -192,6 +192,18 @@ def dist_setup():
     return world, rank, local
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_reference_rate(n: int, budget_s: float = 25.0):
     """Steps/s of the reference's CPU implementation on this host: the
     reference main.c on the oracle's FFT (oracle/_ref/dns) when it exists,
@@ -421,7 +433,8 @@ def run_reference_arm(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"taylor-green {args.n}^3 fp64 nu=1/3000 dt=0.0025",
                    "n": args.n, "nu": NU, "dt": DT},
-        "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -610,7 +623,8 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, cores, kind, sample = cpu_reference_rate(n)
-            cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample}
+            cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sample,
+                   "cpu_model": cpu_model()}
         except Exception as ex:  # the CPU leg is a reported baseline only
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {ex}"}
