@@ -42,8 +42,12 @@ def fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, directions, eps=1e-6, tol=1e-6)
           f"nu rel err {abs(fd - gnu) / abs(gnu):.2e}")
 
 
-def test_adjoint_matches_finite_differences_small(dns):
-    n, nu, dt, nsteps = 16, 0.02, 0.01, 12
+@pytest.mark.parametrize("n", [16, 32])
+def test_adjoint_matches_finite_differences_small(dns, n):
+    """n = 16: the transposed stage takes the velocity and vorticity the
+    forward z pass kept; n = 32 (FP64 with 8 values per thread): it
+    transforms them again."""
+    nu, dt, nsteps = 0.02, 0.01, 12
     u0 = dns.perturbed_tgv(n, seed=5, amplitude=0.3)
     J, g, gnu = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=4)
     assert J == pytest.approx(float(energy(dns, n, *u0, nu, dt, nsteps)), rel=1e-14)
@@ -53,8 +57,9 @@ def test_adjoint_matches_finite_differences_small(dns):
     fd_check(dns, n, u0, nu, dt, nsteps, g, gnu, dirs)
 
 
-def test_adjoint_independent_of_checkpointing(dns):
-    n, nu, dt, nsteps = 16, 0.01, 0.01, 9
+@pytest.mark.parametrize("n", [16, 32])
+def test_adjoint_independent_of_checkpointing(dns, n):
+    nu, dt, nsteps = 0.01, 0.01, 9
     u0 = dns.perturbed_tgv(n, seed=2, amplitude=0.2)
     ref = dns.adjoint_energy(*u0, nu, dt, nsteps, snapshots=20)
     for snaps in (1, 2, 3):
