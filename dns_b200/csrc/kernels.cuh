@@ -447,16 +447,18 @@ struct ZC {
   // after the second and goes through its forward FFT and out before the
   // third; N_x and N_y are then formed in place in the FFT registers.  At
   // most two fields beyond the FFT's own values are live: FP64 keeps (u,
-  // omega_y) in shared memory and (v, omega_x) in registers (64-thread
-  // blocks, 4 per SM: capping the registers for 5 or 6 blocks measured
-  // slower); FP32 keeps both pairs in registers (128 of them).  The first
-  // stage reads the stale velocity where it needs it.
+  // omega_y) in shared memory and (v, omega_x) in registers (128-thread
+  // blocks of 8 lines, 2 per SM, which build the stage twiddles once for 8
+  // lines: 1-10 % faster than 64-thread blocks at 4 per SM; capping the
+  // registers for more blocks measured slower); FP32 keeps both pairs in
+  // registers (128 of them).  The first stage reads the stale velocity
+  // where it needs it.
   static constexpr bool S2 = sizeof(R) == 8 && E >= 16;
   static constexpr bool F32 = sizeof(R) == 4;
-  static constexpr int WANT = S2 ? 64 : 128;
+  static constexpr int WANT = 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
-  static constexpr int MINB = S2 ? 4 : F32 ? 4 : 3;  // blocks per SM
+  static constexpr int MINB = S2 ? 2 : F32 ? 4 : 3;  // blocks per SM
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
   // stage twiddle entries held (even, so the exchange buffers stay 16-byte
