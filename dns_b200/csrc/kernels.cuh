@@ -451,14 +451,15 @@ struct ZC {
   // blocks of 8 lines, 2 per SM, which build the stage twiddles once for 8
   // lines: 1-10 % faster than 64-thread blocks at 4 per SM; capping the
   // registers for more blocks measured slower); FP32 keeps both pairs in
-  // registers (128 of them).  The first stage reads the stale velocity
-  // where it needs it.
+  // registers (128 of them; 512^3 in 256-thread blocks at 2 per SM, 10 %
+  // faster there than 128-thread blocks at 4, 1 % slower at 256^3).  The
+  // first stage reads the stale velocity where it needs it.
   static constexpr bool S2 = sizeof(R) == 8 && E >= 16;
   static constexpr bool F32 = sizeof(R) == 4;
-  static constexpr int WANT = 128;
+  static constexpr int WANT = (F32 && N > 256) ? 256 : 128;
   static constexpr int THREADS = (N * N * T) < WANT ? (N * N * T) : WANT;
   static constexpr int LINES = THREADS / T;
-  static constexpr int MINB = S2 ? 2 : F32 ? 4 : 3;  // blocks per SM
+  static constexpr int MINB = S2 ? 2 : F32 ? (N > 256 ? 2 : 4) : 3;  // blocks per SM
   static constexpr int PADSH = (E >= 16) ? 4 : 3;
   static constexpr int XB = N + (N >> PADSH);     // padded exchange buffer (complex)
   // stage twiddle entries held (even, so the exchange buffers stay 16-byte
