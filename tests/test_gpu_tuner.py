@@ -1,7 +1,8 @@
 """The column-pass autotuner: every register schedule it may pick computes
 bit-identical results (candidates differ only in register allocation), and
 the schedule it reports is the fastest one it timed.  Each candidate is
-forced in a fresh process (the tuner decides once per process and size)."""
+forced in a fresh process (the tuner decides once per process, size and
+batch shape)."""
 import json
 import os
 import subprocess
