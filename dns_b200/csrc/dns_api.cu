@@ -26,6 +26,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <type_traits>
@@ -48,6 +49,25 @@ int fail(int code, const char *what, const char *file, int line) {
   snprintf(buf, sizeof buf, "%s (%s:%d)", what, file, line);
   g_last_error = buf;
   return code;
+}
+
+// Every device allocation of the library goes through here.  Fault
+// injection for the tests of the error paths: with DNS_B200_FAIL_ALLOC=<k>
+// (k >= 1) the k-th allocation of the process fails as an out-of-memory
+// would, before cudaMalloc is called (host side only; nothing runs on the
+// GPU for it).
+std::atomic<long> g_alloc_count{0};
+cudaError_t dev_malloc(void **p, size_t bytes) {
+  static const long fail_at = [] {
+    const char *e = getenv("DNS_B200_FAIL_ALLOC");
+    return e ? atol(e) : 0L;
+  }();
+  const long k = ++g_alloc_count;
+  if (fail_at > 0 && k == fail_at) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
 }
 
 #define CK(call)                                                                     \
@@ -727,7 +747,7 @@ int group_init(Group &G, long n, int precision, unsigned flags, int nruns, cudaS
   const size_t coef_b = (size_t)2 * nruns * sizeof(double);
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   G.arena_bytes = al(spec_b) + al(stale_b) + al(tw_b) + al(part_b) + al(coef_b);
-  cudaError_t e = cudaMalloc((void **)&G.arena, G.arena_bytes);
+  cudaError_t e = dev_malloc((void **)&G.arena, G.arena_bytes);
   if (e != cudaSuccess) {
     G.arena = nullptr;
     return fail(DNS_ERR_NOMEM, cudaGetErrorString(e), __FILE__, __LINE__);
@@ -823,7 +843,7 @@ int init_view(Group &G, int run, cudaStream_t st, bool perturb, unsigned long lo
   double rms = 1.0, scale = 0.0;
   const unsigned blocks = conv_blocks(3 * g.nreal);
   if (perturb) {
-    if (!fp64 && !G.realbuf) CK(cudaMalloc((void **)&G.realbuf, 4 * (size_t)g.nreal * sizeof(double)));
+    if (!fp64 && !G.realbuf) CK(dev_malloc((void **)&G.realbuf, 4 * (size_t)g.nreal * sizeof(double)));
     // FP64: the stale slots hold the noise until its forward transform, then
     // the shaped field; mixed: a float64 buffer
     delta = fp64 ? (double *)V.stale : G.realbuf;
@@ -1277,7 +1297,7 @@ int dns_get_fields(dns_ctx *c, double *U, double *V, double *W, double *P) {
   if (P && !(G.flags & DNS_FLAG_PRESSURE))
     return fail(DNS_ERR_ARG, "P requested without DNS_FLAG_PRESSURE", __FILE__, __LINE__);
   const size_t fb = (size_t)G.g.nreal * sizeof(double);
-  if (!G.realbuf) CK(cudaMalloc((void **)&G.realbuf, 4 * fb));
+  if (!G.realbuf) CK(dev_malloc((void **)&G.realbuf, 4 * fb));
   const int nf = P ? 4 : 3;
   dispatch(G, [&](auto ops) { decltype(ops)::backward(G, c->stream, nf); });
   CKL();
@@ -1432,8 +1452,8 @@ static int ens_build_persistent_t(dns_ens *e) {
   if (per < 1) return fail(DNS_ERR_UNSUPPORTED, "persistent ensemble kernel does not fit", __FILE__, __LINE__);
   e->pgrid = per * sms;
   e->psmem = smem;
-  CK(cudaMalloc(&e->pplan, sizeof plan));
-  CK(cudaMalloc((void **)&e->psync, sizeof(PSync)));
+  CK(dev_malloc(&e->pplan, sizeof plan));
+  CK(dev_malloc((void **)&e->psync, sizeof(PSync)));
   CK(cudaMemcpyAsync(e->pplan, &plan, sizeof plan, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemsetAsync(e->psync, 0, sizeof(PSync), e->stream));
   CK(cudaStreamSynchronize(e->stream));
@@ -1726,7 +1746,7 @@ int dns_selftest_barrier_timeout(double limit_s, int *timed_out) {
   PSync *d = nullptr;
   PSync h{};
   CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  cudaError_t e = cudaMalloc((void **)&d, sizeof(PSync));
+  cudaError_t e = dev_malloc((void **)&d, sizeof(PSync));
   if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(PSync), st);
   if (e == cudaSuccess) e = p_barrier_selftest(d, st, (unsigned long long)(limit_s * 1e9));
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, st);
@@ -1819,7 +1839,7 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     bool zkeep = false;
     dispatch(A.G, [&](auto ops) { zkeep = decltype(ops)::ZKEEP; });
     const size_t keep_a = zkeep ? al(keep_b) : 0;
-    cudaError_t e = cudaMalloc((void **)&A.arena,
+    cudaError_t e = dev_malloc((void **)&A.arena,
                                al(sp_b) + al(re_b) + al(ssp_b) + al(sre_b) + keep_a + al(part_b));
     if (e != cudaSuccess) {
       A.arena = nullptr;
