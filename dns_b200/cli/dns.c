@@ -283,6 +283,32 @@ int main(int argc, char **argv) {
     t = tt;
     tstep += k;
   }
+  /* Opt-in kernel timings (no counterpart in the reference):
+   * DNS_B200_TIMINGS=<k> times k more steps launch by launch after the run
+   * (the printed history is complete before) and prints each kernel's mean
+   * time to stderr. */
+  const char *tenv = getenv("DNS_B200_TIMINGS");
+  if (tenv && atol(tenv) > 0) {
+    static const char *pass[6] = {"A x-inverse", "B y-inverse", "C z-fused",
+                                  "D y-forward", "E1 x-forward", "E2 update"};
+    dns_info_t info;
+    st = dns_get_info(ctx, &info);
+    if (st != DNS_OK)
+      die_status("dns_get_info", st);
+    double *ms = malloc(sizeof(double) * (size_t)info.kernels_per_step);
+    if (!ms)
+      die("out of host memory");
+    st = dns_time_kernels(ctx, nu, dt, atol(tenv), ms);
+    if (st != DNS_OK)
+      die_status("dns_time_kernels", st);
+    double sum = 0.0;
+    for (int q = 0; q < info.kernels_per_step; q++) {
+      fprintf(stderr, "dns: stage %d %s: %.4f ms\n", q / 6, pass[q % 6], ms[q]);
+      sum += ms[q];
+    }
+    fprintf(stderr, "dns: step (sum of its kernels): %.4f ms over %ld steps\n", sum, atol(tenv));
+    free(ms);
+  }
   free(buf);
   dns_destroy(ctx);
   return 0;

@@ -376,3 +376,25 @@ def test_cli_mixed_precision_env(dns, tmp_path):
     bad = subprocess.run([dns.CLI_PATH, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", "0.2"],
                          capture_output=True, text=True, env=dict(os.environ, DNS_B200_PRECISION="fp16"))
     assert bad.returncode == 1 and "DNS_B200_PRECISION" in bad.stderr
+
+
+def test_cli_kernel_timings_env(dns, tmp_path):
+    """DNS_B200_TIMINGS=<k> adds, after the run, one stderr line per kernel
+    of the step (4 stages x 6 passes) with its mean time over k steps; the
+    printed history is the same as without it."""
+    import os
+
+    raw = str(tmp_path / "tgv.raw")
+    dns.write_raw(raw, dns.tgv_fields(32))
+    args = [dns.CLI_PATH, "-i", raw, "-n", "0.01", "-s", "0.01", "-t", "0.2"]
+    env = dict(os.environ)
+    env.pop("DNS_B200_TIMINGS", None)
+    plain = subprocess.run(args, capture_output=True, text=True, env=env)
+    timed = subprocess.run(args, capture_output=True, text=True, env=dict(env, DNS_B200_TIMINGS="3"))
+    assert plain.returncode == 0 and timed.returncode == 0, timed.stderr
+    assert timed.stdout == plain.stdout
+    lines = [l for l in timed.stderr.splitlines() if l.startswith("dns: stage ")]
+    assert len(lines) == 24, timed.stderr
+    times = [float(l.split(": ")[-1].split()[0]) for l in lines]
+    assert all(t > 0 for t in times)
+    assert "over 3 steps" in timed.stderr.splitlines()[-1]
