@@ -97,6 +97,7 @@ _SIGS = {
                                           ctypes.c_int, _P, _P, _P, _P, _P]),
     "dns_adjoint_energy_prec": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, _P, _P, _P, _D, _D,
                                                ctypes.c_long, ctypes.c_int, _P, _P, _P, _P, _P]),
+    "dns_adjoint_schedule": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, _P, _P, _P]),
 }
 
 
@@ -414,6 +415,16 @@ def adjoint_energy(U, V, W, nu: float, dt: float, nsteps: int, snapshots: int = 
                                        snapshots, ctypes.byref(J), _ptr(g[0]), _ptr(g[1]),
                                        _ptr(g[2]), ctypes.byref(gnu)))
     return J.value, tuple(a.reshape(U.shape) for a in g), gnu.value
+
+
+def adjoint_schedule(nsteps: int, snapshots: int):
+    """(forward_steps, recomputed_steps, snapshots_used) of the adjoint's
+    checkpoint schedule (dns_adjoint_schedule; host only)."""
+    lib = load_library()
+    f, rc, used = ctypes.c_long(), ctypes.c_long(), ctypes.c_int()
+    _check(lib.dns_adjoint_schedule(nsteps, snapshots, ctypes.byref(f), ctypes.byref(rc),
+                                    ctypes.byref(used)))
+    return f.value, rc.value, used.value
 
 
 def final_energy(U, V, W, nu: float, dt: float, nsteps: int,

@@ -1125,49 +1125,78 @@ long adj_split(long a, long b, int free) {
   return b - lr;
 }
 
+// The checkpoint schedule below drives an executor: AdjDev runs it on the
+// device, AdjCount only counts it (dns_adjoint_schedule).
+struct AdjDev {
+  Adj &A;
+  int advance(long m) { return adj_advance(A, m); }
+  int store(int k) { return adj_snap_store(A, k); }
+  int restore(int k) { return adj_snap_restore(A, k); }
+  int step_one() { return adj_step_one(A); }
+};
+struct AdjCount {
+  long advanced = 0, reversed = 0;
+  int used = 1;  // snapshot 0 holds the initial state
+  int advance(long m) {
+    advanced += m;
+    return DNS_OK;
+  }
+  int store(int k) {
+    used = k + 1 > used ? k + 1 : used;
+    return DNS_OK;
+  }
+  int restore(int) { return DNS_OK; }
+  int step_one() {
+    reversed++;
+    return DNS_OK;
+  }
+};
+
 // forward sweep over steps [0, b) from the state in snapshot 0, storing
 // the snapshots of the reverse sweep's rightmost path (the split points
 // adj_reverse takes first, each with one snapshot fewer) on the way, so
 // the reverse sweep need not recompute them
-int adj_sweep(Adj &A, long b, int free) {
+template <class Ex>
+int adj_sweep(Ex &x, long b, int free) {
   long a = 0;
   int ka = 0, r;
   while (b - a >= 2 && free >= 1) {
     const long m = adj_split(a, b, free);
-    if ((r = adj_advance(A, m - a))) return r;
-    if ((r = adj_snap_store(A, ka + 1))) return r;
+    if ((r = x.advance(m - a))) return r;
+    if ((r = x.store(ka + 1))) return r;
     a = m;
     ka++;
     free--;
   }
-  return adj_advance(A, b - a);
+  return x.advance(b - a);
 }
 
 // reverse steps [a, b): the state at step a is in snapshot ka; snapshots
 // ka+1 .. ka+free are unused, unless `stored`: then those of the rightmost
 // path of the split tree are already in place (adj_sweep)
-int adj_reverse(Adj &A, long a, long b, int ka, int free, bool stored) {
+template <class Ex>
+int adj_reverse(Ex &x, long a, long b, int ka, int free, bool stored) {
   int r;
   if (b - a == 1) {
-    if ((r = adj_snap_restore(A, ka))) return r;
-    return adj_step_one(A);
+    if ((r = x.restore(ka))) return r;
+    return x.step_one();
   }
   if (free == 0) {  // no snapshot to spare: recompute from a for every step
     for (long t = b - 1; t >= a; t--) {
-      if ((r = adj_snap_restore(A, ka))) return r;
-      if ((r = adj_advance(A, t - a))) return r;
-      if ((r = adj_step_one(A))) return r;
+      if ((r = x.restore(ka))) return r;
+      if ((r = x.advance(t - a))) return r;
+      if ((r = x.step_one())) return r;
     }
     return DNS_OK;
   }
   const long m = adj_split(a, b, free);
   if (!stored) {
-    if ((r = adj_snap_restore(A, ka))) return r;
-    if ((r = adj_advance(A, m - a))) return r;
-    if ((r = adj_snap_store(A, ka + 1))) return r;
+    if ((r = x.restore(ka))) return r;
+    if ((r = x.advance(m - a))) return r;
+    if ((r = x.store(ka + 1))) return r;
   }
-  if ((r = adj_reverse(A, m, b, ka + 1, free - 1, stored))) return r;
-  return adj_reverse(A, a, m, ka, free, false);
+  if ((r = adj_reverse(x, m, b, ka + 1, free - 1, stored))) return r;
+  return adj_reverse(x, a, m, ka, free, false);
 }
 
 int ctx_build_graph(dns_ctx *c) {
@@ -1880,7 +1909,11 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
   if (r == DNS_OK) r = set_velocity_view(A.G, A.st, U, V, W);
   if (r == DNS_OK) r = adj_snap_store(A, 0);
   if (r == DNS_OK)  // forward sweep to T
-    r = want_grad ? adj_sweep(A, nsteps, snapshots - 1) : adj_advance(A, nsteps);
+    r = want_grad ? [&] {
+      AdjDev x{A};
+      return adj_sweep(x, nsteps, snapshots - 1);
+    }()
+                  : adj_advance(A, nsteps);
   double4 d = make_double4(0, 0, 0, 0);
   const double invn3 = 1.0 / (double)g.nreal;
   if (r == DNS_OK) {
@@ -1905,7 +1938,10 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
     cudaError_t e = cudaMemsetAsync(A.Rf(RE_LSTALE), 0, A.real3d(), A.st);
     if (e != cudaSuccess) r = fail(DNS_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
   }
-  if (r == DNS_OK) r = adj_reverse(A, 0, nsteps, 0, snapshots - 1, true);
+  if (r == DNS_OK) {
+    AdjDev x{A};
+    r = adj_reverse(x, 0, nsteps, 0, snapshots - 1, true);
+  }
   if (r == DNS_OK) {
     // dE/du0 = r2c^T(lambda_U(0)) + lambda_stale(0) = c2r(lambda / w_z) + lambda_stale
     const int t3[3] = {0, 1, 2};
@@ -1931,6 +1967,20 @@ int dns_adjoint_energy_prec(long n, int precision, const double *U, const double
   }
   cleanup();
   return r;
+}
+
+int dns_adjoint_schedule(long nsteps, int snapshots, long *forward_steps, long *recomputed_steps,
+                         int *snapshots_used) {
+  if (nsteps < 1 || snapshots < 1)
+    return fail(DNS_ERR_ARG, "nsteps and snapshots must be >= 1", __FILE__, __LINE__);
+  AdjCount x;
+  adj_sweep(x, nsteps, snapshots - 1);
+  const long sweep = x.advanced;
+  adj_reverse(x, 0, nsteps, 0, snapshots - 1, true);
+  if (forward_steps) *forward_steps = x.advanced;
+  if (recomputed_steps) *recomputed_steps = x.advanced - sweep;
+  if (snapshots_used) *snapshots_used = x.used;
+  return DNS_OK;
 }
 
 int dns_adjoint_energy(long n, const double *U, const double *V, const double *W, double nu,

@@ -245,6 +245,16 @@ int dns_adjoint_energy(long n, const double *U, const double *V, const double *W
 int dns_adjoint_energy_prec(long n, int precision, const double *U, const double *V,
                             const double *W, double nu, double dt, long nsteps, int snapshots,
                             double *J, double *gU, double *gV, double *gW, double *gnu);
+/* The checkpoint schedule the two calls above follow for nsteps steps and
+ * `snapshots` stored states, counted on the host (no GPU work; callable
+ * without a GPU), to choose `snapshots` against time: forward_steps = the
+ * steps of the first sweep (nsteps) plus those recomputed from snapshots
+ * (recomputed_steps); each reversed step then re-runs its own stages once
+ * more.  snapshots_used <= snapshots.  With snapshots >= nsteps nothing is
+ * recomputed; with 1, every step is recomputed from the start (nsteps *
+ * (nsteps - 1) / 2).  Any output pointer may be NULL. */
+int dns_adjoint_schedule(long nsteps, int snapshots, long *forward_steps, long *recomputed_steps,
+                         int *snapshots_used);
 
 /* Energy and enstrophy of a spectral velocity held in caller-owned device
  * memory, allocating nothing.  No counterpart in the reference (main.c has

@@ -180,3 +180,60 @@ def test_counter_normals_match_scalar_restatement_and_are_normal():
     assert abs(x.mean()) < 5e-3 and abs(x.std() - 1) < 5e-3
     assert np.array_equal(x[:100], dns_b200.counter_normals(3, 0, 100))  # a counter, not a state
     assert not np.allclose(x[:100], dns_b200.counter_normals(3, 1, 100))
+
+
+def _schedule_restated(nsteps, snapshots):
+    """The binomial checkpoint schedule restated: (forward, recomputed)."""
+    from math import comb
+
+    cnt = {"adv": 0}
+
+    def split(a, b, free):
+        l, rr = b - a, 0
+        while comb(free + rr, free) < l:
+            rr += 1
+        return b - max(min(comb(free - 1 + rr, free - 1), l - 1), 1)
+
+    def rev(a, b, free, stored):
+        if b - a == 1:
+            return
+        if free == 0:
+            cnt["adv"] += sum(t - a for t in range(a, b))
+            return
+        m = split(a, b, free)
+        if not stored:
+            cnt["adv"] += m - a
+        rev(m, b, free - 1, stored)
+        rev(a, m, free, False)
+
+    rev(0, nsteps, snapshots - 1, True)
+    return nsteps + cnt["adv"], cnt["adv"]
+
+
+@pytest.mark.parametrize("nsteps,snapshots", [(401, 20), (401, 1), (401, 2), (401, 401),
+                                              (12, 4), (9, 3), (1, 1), (1000, 7)])
+def test_adjoint_schedule_counts(dns_lib, nsteps, snapshots):
+    """dns_adjoint_schedule (host only) counts the schedule the adjoint
+    runs: against a restatement, the known cases (one snapshot recomputes
+    every step from the start; enough snapshots recompute nothing), and
+    never more snapshots than given."""
+    import dns_b200
+
+    fwd, rec, used = dns_b200.adjoint_schedule(nsteps, snapshots)
+    assert (fwd, rec) == _schedule_restated(nsteps, snapshots)
+    assert fwd == nsteps + rec and 1 <= used <= snapshots
+    if snapshots == 1:
+        assert rec == nsteps * (nsteps - 1) // 2
+    if snapshots >= nsteps:
+        assert rec == 0
+    if (nsteps, snapshots) == (401, 20):
+        assert rec == 684
+
+
+def test_adjoint_schedule_more_snapshots_recompute_less(dns_lib):
+    import dns_b200
+
+    recs = [dns_b200.adjoint_schedule(401, s)[1] for s in range(1, 40)]
+    assert all(a >= b for a, b in zip(recs, recs[1:]))
+    with pytest.raises(dns_b200.DNSError):
+        dns_b200.adjoint_schedule(0, 3)
