@@ -8,7 +8,9 @@ the CPU-baseline leg of bench.py use it, always as the checker; the product
 
 Parity pin: the oracle and oracle/_ref/dns (the reference main.c compiled
 unchanged against the same shim) reproduce the reference's own golden
-histories 0128/* and 0256/* (tests/golden); see tests/test_oracle.py.
+histories 0128/* and 0256/* (tests/golden); see tests/test_oracle.py.  A
+second restatement on numpy's FFT (oracle/numpy_restatement.py) agrees with
+the C one step by step, which pins the shim FFT independently.
 """
 from __future__ import annotations
 
